@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the SU(N) heatbath/overrelaxation sweep on B200.
+
+Workload (one "step" = one sweep): SU(3) 32^4, beta = 6.0, Haar hot start,
+FP32 links in 12-parameter even/odd SoA, 1 heatbath + 4 overrelaxation passes
+per sweep, FP64 reunitarization every 10 sweeps.  One sweep is 20 V link
+updates.  The metric is link-updates/s, whole job (all ranks).
+
+Multi-GPU: independent lattices per rank ("replicas only": the path does not
+shard), max-over-ranks device time.
+
+--impl reference times the reference algorithm's CPU implementation (the
+FP64 oracle port, all host threads) on a bounded sample of the same sweep.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (32, 32, 32, 32)
+BETA = 6.0
+N = 3
+SEED = 1234
+REUNIT = 10
+WORKLOAD = ("SU(3) 32^4 beta=6.0 Haar hot start, FP32 SOA12 even/odd links, 1 HB + 4 OR per sweep, "
+            "FP64 reunitarization every 10 sweeps")
+LINK_RECORD = {"SOA12_f32": 48, "SOA_f64": 144, "SOA_f32": 72}
+
+
+def measured_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_sample(nthreads=0, reps=1, lattice=None):
+    """Oracle (FP64 C, OpenMP) on 1/8 of a sweep with the sweep's mix: one
+    heatbath and four overrelaxation phases of (parity 0, mu 0) on the full
+    lattice.  Returns (link-updates/s, threads, seconds)."""
+    from oracle import oracle as O
+    X = list(DIMS)
+    U = lattice if lattice is not None else O.hot(N, X, SEED)
+    V = O.volume(X)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        O.update_phase(U, X, 0, 0, 0, BETA, O.RNG_PHILOX32, SEED, 0, nthreads=nthreads)
+        for _ in range(4):
+            O.update_phase(U, X, 0, 0, 1, BETA, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    threads = nthreads or (os.cpu_count() or 1)
+    return reps * 5 * (V // 2) / dt, threads, dt
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.build() if not os.path.exists(os.path.join(ROOT, "oracle", "libsun_oracle.so")) else None
+    U = O.hot(N, list(DIMS), SEED)
+    for _ in range(args.warmup):
+        cpu_sample(lattice=U)
+    rates, tot = [], 0.0
+    for _ in range(args.steps):
+        r, threads, dt = cpu_sample(lattice=U)
+        rates.append(r)
+        tot += dt
+    V = O.volume(list(DIMS))
+    value = args.steps * 5 * (V // 2) / tot
+    line = {
+        "metric": "link-updates/s", "value": value, "unit": "link-updates/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Haar hot start)", "impl": "reference",
+        "config": {"workload": WORKLOAD, "lattice": list(DIMS), "parallelism": "replicas"},
+        "cpu_baseline": {"value": value, "unit": "link-updates/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "1/8 sweep per step: one heatbath + four overrelaxation phases (parity 0, mu 0) "
+                                   "over the full 32^4 lattice, FP64 oracle, OpenMP over sites"},
+        "e2e": {"value": value, "unit": "link-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP64 and batched side measurements")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from sun_b200 import Context, gauge
+    from sun_b200._native import check, lib
+    L = lib()
+
+    ctx = Context(local)
+    stream = torch.cuda.Stream()
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    V = DIMS[0] * DIMS[1] * DIMS[2] * DIMS[3]
+    g = gauge(ctx, N=N, dims=DIMS, beta=BETA, atype=1, evenodd=True, prec="f32", seed=SEED + rank,
+              reunit_every=REUNIT)
+    g.Init(hot=True)
+
+    def sweeps(lat, n):
+        check(L.sun_sweep(lat.h, 1, 4, n, sp), ctx.h)
+
+    # warm-up
+    sweeps(g, args.warmup)
+    stream.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sweeps(g, args.steps)
+    e1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    t_main = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+
+    # dominant kernel: the overrelaxation phase launch (32 of the 40 update
+    # launches of a sweep); 8 launches per pass
+    n_or = 10
+    e0.record(stream)
+    check(L.sun_overrelax(g.h, n_or, sp), ctx.h)
+    e1.record(stream)
+    stream.synchronize()
+    t_or = e0.elapsed_time(e1) / 1e3 / (8 * n_or)
+    n_hbp = 4
+    e0.record(stream)
+    check(L.sun_heatbath(g.h, n_hbp, sp), ctx.h)
+    e1.record(stream)
+    stream.synchronize()
+    t_hb = e0.elapsed_time(e1) / 1e3 / (8 * n_hbp)
+    clk = clocks.stop()
+
+    # end to end through the C ABI with host buffers: upload the image from
+    # pinned memory, one sweep, plaquette to the host, download the image
+    img_bytes = g.Bytes()
+    host = torch.empty(img_bytes, dtype=torch.uint8, pin_memory=True)
+    check(L.sun_lattice_download(g.h, C.c_void_p(host.data_ptr()), 1, sp), ctx.h)
+    plq = (C.c_double * 2)()
+    k_e2e = max(3, min(args.steps, 10))
+    for _ in range(2):
+        check(L.sun_lattice_upload(g.h, C.c_void_p(host.data_ptr()), 1, sp), ctx.h)
+        sweeps(g, 1)
+        check(L.sun_plaquette(g.h, plq, sp), ctx.h)
+        check(L.sun_lattice_download(g.h, C.c_void_p(host.data_ptr()), 1, sp), ctx.h)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(k_e2e):
+        check(L.sun_lattice_upload(g.h, C.c_void_p(host.data_ptr()), 1, sp), ctx.h)
+        sweeps(g, 1)
+        check(L.sun_plaquette(g.h, plq, sp), ctx.h)
+        check(L.sun_lattice_download(g.h, C.c_void_p(host.data_ptr()), 1, sp), ctx.h)
+    e1.record(stream)
+    stream.synchronize()
+    barrier()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+
+    extras = {}
+    if not args.no_extras:
+        # plain single-lattice FP64 full-link sweep (the denominator of the
+        # batched-vs-plain target)
+        g64 = gauge(ctx, N=N, dims=DIMS, beta=BETA, atype=0, evenodd=True, prec="f64", seed=SEED,
+                    reunit_every=REUNIT)
+        g64.Init(hot=True)
+        sweeps(g64, 3)
+        k64 = max(3, args.steps // 3)
+        stream.synchronize()
+        e0.record(stream)
+        sweeps(g64, k64)
+        e1.record(stream)
+        stream.synchronize()
+        t64 = e0.elapsed_time(e1) / 1e3
+        extras["fp64_soa_plain"] = {"value": 20 * V * k64 / t64, "unit": "link-updates/s", "sweeps": k64,
+                                    "hbm_gbs_model": 20 * V * k64 * 9 * 144 / t64 / 1e9}
+        g64.Release()
+        extras["batched"] = batched_bench(ctx, L, sp, stream, args)
+
+    line = {
+        "metric": "link-updates/s",
+        "value": world * 20 * V * args.steps / t_main,
+        "unit": "link-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_main / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded Haar hot start, Philox stream)",
+        "config": {"workload": WORKLOAD, "lattice": list(DIMS), "ncolors": N, "beta": BETA, "layout": "SOA12",
+                   "precision": "f32", "order": "even/odd", "sweep": "1 HB + 4 OR", "reunit_every": REUNIT,
+                   "step": "one sweep = 20 V link updates",
+                   "l2": "inputs larger than L2 (201 MB link image vs 126 MB L2)", "parallelism": "replicas"},
+        "gpu_launches": args.steps * 42,
+        "clocks": clk,
+    }
+    peak, peak_kind = measured_hbm()
+    bytes_or = (V // 2) * 9 * LINK_RECORD["SOA12_f32"]
+    ach = bytes_or / t_or / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_update_or_f32_soa12_32x4.json")) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+    except Exception:
+        pass
+    line["roofline"] = {"bound": "hbm", "kernel": "k_update<3,float,SOA12,OR>", "achieved": ach, "peak": peak,
+                        "unit": "GB/s", "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind,
+                        "launch_us": t_or * 1e6, "algorithmic_bytes_per_launch": bytes_or,
+                        "hb_launch_us": t_hb * 1e6, "hb_achieved_gbs": bytes_or / t_hb / 1e9}
+    line["e2e"] = {"value": world * 20 * V * k_e2e / t_e2e, "unit": "link-updates/s",
+                   "h2d_bytes_per_step": img_bytes, "d2h_bytes_per_step": img_bytes + 16,
+                   "step": "upload image (pinned) + 1 sweep + plaquette + download image, C ABI"}
+    line.update(extras)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, threads, dt = cpu_sample()
+        line["cpu_baseline"] = {"value": rate, "unit": "link-updates/s", "cores": threads, "kind": "port",
+                                "sample": f"1/8 sweep (one heatbath + four overrelaxation phases, parity 0 mu 0) "
+                                          f"of the 32^4 lattice, FP64 oracle, {dt:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.Release()
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def batched_bench(ctx, L, sp, stream, args):
+    """64 independent SU(3) lattices, L in {8,12,16}, T in {L,2L}, beta in
+    [5.7,6.4], FP32 SOA12, advanced together from a captured CUDA graph."""
+    import numpy as np
+    import torch
+    from sun_b200 import Batch, gauge
+    from sun_b200._native import check
+    rng = np.random.default_rng(1234)
+    lats, vol = [], 0
+    b = Batch(ctx)
+    for i in range(64):
+        l = int(rng.choice([8, 12, 16]))
+        t = int(rng.choice([l, 2 * l]))
+        beta = float(rng.uniform(5.7, 6.4))
+        g = gauge(ctx, N=3, dims=(l, l, l, t), beta=beta, atype=1, evenodd=True, prec="f32", seed=1234 + 7919 * i,
+                  reunit_every=10)
+        g.Init(hot=True)
+        b.add(g)
+        lats.append(g)
+        vol += l ** 3 * t
+    check(L.sun_batch_sweep(b.h, 1, 4, 3, 1, sp), ctx.h)
+    k = max(5, args.steps)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream.synchronize()
+    e0.record(stream)
+    check(L.sun_batch_sweep(b.h, 1, 4, k, 1, sp), ctx.h)
+    e1.record(stream)
+    stream.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    rate = 20 * vol * k / t
+    out = {"value": rate, "unit": "link-updates/s", "lattices": 64, "total_sites": vol, "sweeps": k,
+           "hbm_gbs_model": rate * 9 * 48 / 1e9, "graph": True}
+    b.close()
+    for g in lats:
+        g.Release()
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,198 @@
+/*
+ * sun_b200.h -- C ABI of the B200-native SU(N) quenched lattice gauge engine.
+ *
+ * Drop-in boundary for the hot path of nmrcardoso/sun (CULQCD): gauge-array
+ * allocation and layouts, the heatbath / overrelaxation Monte Carlo sweep,
+ * reunitarization, and plaquette / Polyakov-loop / Wilson-loop measurements,
+ * plus batched many-lattice execution and a continuous-batching server on one
+ * GPU.  Each declaration names the reference interface it replaces
+ * (paths relative to the reference project root).
+ *
+ * Conventions
+ *  - Every call returns a sun_status; nothing here calls exit() (the
+ *    reference's errorCULQCD / CUDA_SAFE_CALL exit the process,
+ *    include/comm_mpi.h:102-116, include/cuda_common.h:136-205).
+ *    sun_last_error_string() gives the message of the last failure.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the context stream).
+ *    Calls that return host values synchronise that stream.
+ *  - The library owns all device memory; callers own handles.
+ *  - Host lattice buffers: SUN_HOST_CANONICAL is double complex
+ *    U[V][4][N][N] with sites in x-fastest lexicographic order, the record
+ *    order of the reference gauge file (src/io_gauge.cpp:544-563);
+ *    SUN_HOST_IMAGE is the raw device image (layout, order and precision of
+ *    the lattice), what a reference `gauge` in Host mode holds.
+ */
+#ifndef SUN_B200_H
+#define SUN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SUN_OK = 0,
+    SUN_ERR_INVALID_ARG = 1,
+    SUN_ERR_UNSUPPORTED = 2,
+    SUN_ERR_OUT_OF_MEMORY = 3,
+    SUN_ERR_CUDA = 4,
+    SUN_ERR_IO = 5,
+    SUN_ERR_STATE = 6,
+    SUN_ERR_CAPACITY = 7,
+    SUN_ERR_DEVICE_FLAG = 8
+} sun_status;
+
+/* ArrayType (include/modes.h:66-71): SOA = N*N complex, SOA12 = 2 rows (SU(3)),
+ * SOA8 = 8 reals (SU(3)).  SOA12A (anti-Hermitian storage for gauge fixing) is
+ * out of scope. */
+typedef enum { SUN_SOA = 0, SUN_SOA12 = 1, SUN_SOA8 = 2 } sun_layout;
+typedef enum { SUN_EVEN_ODD = 0, SUN_NORMAL = 1 } sun_order;
+typedef enum { SUN_F32 = 0, SUN_F64 = 1 } sun_precision;
+typedef enum { SUN_HOST_CANONICAL = 0, SUN_HOST_IMAGE = 1 } sun_host_format;
+
+typedef struct sun_ctx sun_ctx;
+typedef struct sun_lattice sun_lattice;
+typedef struct sun_batch sun_batch;
+typedef struct sun_server sun_server;
+
+typedef struct {
+    int device;            /* CUDA device ordinal (initCULQCD gpuid) */
+    int verbosity;         /* 0 silent .. 3 debug (Verbosity, include/modes.h:74-79) */
+    int tune;              /* 1: autotune launch shapes (TuneMode) */
+    const char *tune_cache_path; /* CSV cache file, NULL: none ($CULQCD_RESOURCE_PATH/tunecache.csv) */
+    size_t hbm_budget_bytes;     /* admission budget for the server; 0: 90% of free memory */
+} sun_config;
+
+typedef struct {
+    int ncolors;           /* N in {2,3,4,6} (the reference's compile-time NCOLORS, Makefile:6) */
+    int dims[4];           /* X, Y, Z, T; all even (constants.cu:170-174) */
+    double beta;
+    sun_layout layout;
+    sun_order order;
+    sun_precision precision;
+    uint64_t seed;         /* Philox key of this lattice */
+    int reunit_every;      /* FP64 reunitarization every k sweeps inside sun_sweep (0: never) */
+} sun_lattice_params;
+
+/* ---- lifecycle: initCULQCD / EndCULQCD (src/comm_mpi.cpp:107, :186) ---- */
+sun_status sun_init(const sun_config *cfg, sun_ctx **out);
+sun_status sun_finalize(sun_ctx *ctx);
+const char *sun_last_error_string(const sun_ctx *ctx);
+const char *sun_version(void);
+
+/* ---- gauge arrays: _gauge<Real>(ArrayType, Device, 4V, evenodd) + Allocate
+ * (include/gaugearray.h:139, :603) with SETPARAMS geometry
+ * (src/constants.cu:149) made per-lattice. ---- */
+sun_status sun_lattice_create(sun_ctx *ctx, const sun_lattice_params *p, sun_lattice **out);
+sun_status sun_lattice_destroy(sun_lattice *lat);
+sun_status sun_lattice_bytes(const sun_lattice *lat, size_t *bytes);
+/* raw device pointer of the image (the reference's gauge::GetPtr) */
+sun_status sun_lattice_device_ptr(const sun_lattice *lat, void **dptr);
+/* ColdStart / HotStart (src/gaugearray.cu:290, :388); the hot start is Haar */
+sun_status sun_lattice_init_cold(sun_lattice *lat, void *stream);
+sun_status sun_lattice_init_hot(sun_lattice *lat, void *stream);
+/* host <-> device (gauge::Copy + cudaMemcpy of the reference) */
+sun_status sun_lattice_upload(sun_lattice *lat, const void *host, sun_host_format fmt, void *stream);
+sun_status sun_lattice_download(sun_lattice *lat, void *host, sun_host_format fmt, void *stream);
+/* layout / order / precision conversion, gauge::Copy (src/gaugearray.cu:130) */
+sun_status sun_lattice_copy(sun_lattice *dst, sun_lattice *src, void *stream);
+/* RNG state for checkpoint: RNG::Save / RNG::Read (src/random.cu:164, :183);
+ * with Philox the state is (seed, heatbath-pass counter, sweep counter) */
+sun_status sun_lattice_get_rng(sun_lattice *lat, uint64_t *seed, uint32_t *hb_passes, uint32_t *sweeps);
+sun_status sun_lattice_set_rng(sun_lattice *lat, uint64_t seed, uint32_t hb_passes, uint32_t sweeps);
+
+/* ---- Monte Carlo: HeatBath<Real>::Run (src/monte/monte.cu:196),
+ * OverRelaxation<Real>::Run (src/monte/ovr.cu:182).  Even/odd arrays only,
+ * like the reference kernels. ---- */
+sun_status sun_heatbath(sun_lattice *lat, int n_passes, void *stream);
+sun_status sun_overrelax(sun_lattice *lat, int n_passes, void *stream);
+/* n_sweeps x (n_hb heatbath + n_or overrelaxation); reunitarizes after every
+ * reunit_every-th sweep (lattice parameter) */
+sun_status sun_sweep(sun_lattice *lat, int n_hb, int n_or, int n_sweeps, void *stream);
+/* one heatbath pass fed caller uniforms (oracle parity): device buffer
+ * u[(lex*4 + mu)*stride + k]; running out sets SUN_ERR_DEVICE_FLAG */
+sun_status sun_heatbath_injected(sun_lattice *lat, const double *dev_uniforms, int stride, void *stream);
+
+/* ---- Reunitarize<Real>::Run (src/reunitarize.cu:78), FP64 arithmetic ---- */
+sun_status sun_reunitarize(sun_lattice *lat, void *stream);
+/* max over links of max_ij |(U^dag U - 1)_ij| */
+sun_status sun_unitarity_violation(sun_lattice *lat, double *out, void *stream);
+
+/* ---- measurements (FP64 results, deterministic compensated sums) ----
+ * PlaquetteCUB<Real>::Run -> {spatial, temporal} (src/meas/plaquette_cub.cu:226)
+ * OnePolyakovLoop<Real>::Run -> {re, im} (src/meas/polyakovloop.cu:637)
+ * WilsonLoop<Real>(gauge, res, R, T) -> res[t + r(T+1)] complex
+ *   (src/meas/wilsonloop.cu:535); R, T <= 8; any storage order accepted. */
+sun_status sun_plaquette(sun_lattice *lat, double out[2], void *stream);
+sun_status sun_polyakov(sun_lattice *lat, double out[2], void *stream);
+sun_status sun_wilson_loops(sun_lattice *lat, int R, int T, double *out, void *stream);
+
+/* ---- gauge file: SaveBin_Gauge<Real,RealSave> / ReadBin_Gauge
+ * (src/io_gauge.cpp:429, :605), byte-compatible; save_fp64 selects RealSave,
+ * the header's beta field has the lattice's own precision ---- */
+sun_status sun_save_bin(sun_lattice *lat, const char *path, int save_fp64, int with_header);
+sun_status sun_load_bin(sun_lattice *lat, const char *path, int save_fp64, int with_header);
+
+/* ---- batches: many lattices of any (N, precision, layout) advanced by one
+ * launch per (class, phase); no reference counterpart (one lattice per
+ * process there) ---- */
+sun_status sun_batch_create(sun_ctx *ctx, sun_batch **out);
+sun_status sun_batch_destroy(sun_batch *b);
+sun_status sun_batch_add(sun_batch *b, sun_lattice *lat);
+sun_status sun_batch_remove(sun_batch *b, sun_lattice *lat);
+sun_status sun_batch_size(const sun_batch *b, int *n);
+/* use_graph: capture one sweep into a CUDA graph and replay it */
+sun_status sun_batch_sweep(sun_batch *b, int n_hb, int n_or, int n_sweeps, int use_graph, void *stream);
+/* out[2*i], out[2*i+1] for the i-th lattice in insertion order */
+sun_status sun_batch_plaquette(sun_batch *b, double *out, void *stream);
+sun_status sun_batch_polyakov(sun_batch *b, double *out, void *stream);
+
+/* ---- continuous-batching server ---- */
+typedef struct {
+    int ncolors;
+    int dims[4];
+    double beta;
+    int sweeps;            /* sweeps of (n_hb heatbath + n_or overrelaxation) */
+    int n_hb, n_or;
+    uint64_t seed;
+    int hot_start;         /* 1 Haar, 0 cold */
+    int observables;       /* bit 0 plaquette, bit 1 Polyakov, bit 2 Wilson loops */
+    int wilson_R, wilson_T;
+    sun_precision precision;
+    sun_layout layout;
+    int reunit_every;
+} sun_job;
+
+typedef struct {
+    int64_t id;
+    int status;            /* sun_status of the job */
+    double plaquette[2];
+    double polyakov[2];
+    double wilson[2 * 9 * 9];
+    double submit_s, start_s, finish_s;  /* server clock */
+    double link_updates;
+} sun_result;
+
+sun_status sun_server_create(sun_ctx *ctx, int max_active, sun_server **out);
+sun_status sun_server_destroy(sun_server *s);
+/* queue a job; the server admits it when its HBM footprint fits */
+sun_status sun_server_submit(sun_server *s, const sun_job *job, int64_t *id);
+/* run one scheduling step: admit, advance every active job by one sweep,
+ * retire finished jobs; *n_done results are written to out[0..cap) */
+sun_status sun_server_step(sun_server *s, sun_result *out, int cap, int *n_done);
+sun_status sun_server_pending(const sun_server *s, int *queued, int *active);
+/* bytes a job needs on the device (links + measurement scratch) */
+sun_status sun_job_footprint(const sun_job *job, size_t *bytes);
+/* override the admission budget (default 85% of free device memory) */
+sun_status sun_server_set_budget(sun_server *s, size_t bytes);
+/* the admission rule: how many of the queued jobs (FIFO, footprints given)
+ * to admit with `free_slots` slots and `used` of `budget` bytes taken */
+sun_status sun_admit_count(const size_t *footprints, int n_queued, size_t budget, size_t used, int free_slots,
+                           int *n_admit);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

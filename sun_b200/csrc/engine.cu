@@ -1,0 +1,1035 @@
+// engine.cu -- host runtime and C ABI of the engine (include/sun_b200.h).
+//
+// Objects: a context (device, stream, last error, launch shapes), lattices
+// (device image + device-resident RNG/sweep counters), groups (device tables
+// of same-class lattices that one launch advances), batches (groups of
+// mixed classes, optionally replayed from a CUDA graph) and a server
+// (continuous batching over a batch).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sun_b200.h"
+#include "sun_ops.h"
+
+using namespace sunb;
+
+namespace {
+
+struct Error : std::runtime_error {
+    sun_status st;
+    Error(sun_status s, const std::string& m) : std::runtime_error(m), st(s) {}
+};
+
+[[noreturn]] void fail(sun_status st, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    throw Error(st, buf);
+}
+
+void ck(cudaError_t e, const char* what)
+{
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        fail(SUN_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    }
+    if (e != cudaSuccess) fail(SUN_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Device buffer owned by the library.
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void ensure(size_t bytes)
+    {
+        if (bytes <= n) return;
+        release();
+        ck(cudaMalloc(&p, bytes), "cudaMalloc");
+        n = bytes;
+    }
+};
+
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    ~PinnedBuf()
+    {
+        if (p) cudaFreeHost(p);
+    }
+    void ensure(size_t bytes)
+    {
+        if (bytes <= n) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        ck(cudaMallocHost(&p, bytes), "cudaMallocHost");
+        n = bytes;
+    }
+};
+
+int elems_of(int N, int layout)
+{
+    if (layout == SUN_SOA12) return 6;
+    if (layout == SUN_SOA8) return 4;
+    return N * N;
+}
+
+double now_s()
+{
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct sun_ctx {
+    int device = 0;
+    int verbosity = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    std::recursive_mutex mu;
+    DevBuf err;          // device error word (injected-stream overrun)
+    size_t hbm_budget = 0;
+    // launch shapes (CTA sizes) per kernel family
+    int blk_update = 128, blk_sites = 128, blk_links = 256, blk_wilson = 64;
+};
+
+namespace { struct Group; }
+
+struct sun_lattice {
+    sun_ctx* ctx = nullptr;
+    sun_lattice_params p{};
+    DevBuf links;
+    DevBuf state;        // uint32 [heatbath passes, sweeps]
+    size_t bytes = 0;
+    LatDev desc{};
+    unsigned version = 0;    // bumped when desc changes (device tables re-upload)
+    Group* solo = nullptr;   // one-lattice launch table, built on first use
+    ~sun_lattice();
+};
+
+namespace {
+
+cudaStream_t S(sun_ctx* c, void* s) { return s ? reinterpret_cast<cudaStream_t>(s) : c->stream; }
+
+int work_of(const LatDev& L, int kind)
+{
+    switch (kind) {
+    case WORK_HALF: return L.halfV;
+    case WORK_SITES: return L.V;
+    case WORK_SPATIAL: return L.X[0] * L.X[1] * L.X[2];
+    default: return 4 * L.V;
+    }
+}
+
+// Same-class lattices advanced by one launch per kernel.
+struct Group {
+    int N = 0, fp64 = 0, layout = 0;
+    std::vector<sun_lattice*> lats;
+    DevBuf d_lats;
+    std::map<std::pair<int, int>, std::pair<std::shared_ptr<DevBuf>, int>> begins;
+    DevBuf partials, out;
+    PinnedBuf h_out;
+    bool dirty = true;
+    std::vector<unsigned> versions;
+
+    void sync(cudaStream_t s)
+    {
+        if (!dirty) {
+            for (size_t i = 0; i < lats.size(); ++i)
+                if (versions[i] != lats[i]->version) dirty = true;
+        }
+        if (!dirty) return;
+        std::vector<LatDev> h(lats.size());
+        versions.resize(lats.size());
+        for (size_t i = 0; i < lats.size(); ++i) {
+            h[i] = lats[i]->desc;
+            versions[i] = lats[i]->version;
+        }
+        d_lats.ensure(sizeof(LatDev) * std::max<size_t>(1, h.size()));
+        if (!h.empty())
+            ck(cudaMemcpyAsync(d_lats.p, h.data(), sizeof(LatDev) * h.size(), cudaMemcpyHostToDevice, s),
+               "table upload");
+        ck(cudaStreamSynchronize(s), "table upload");
+        begins.clear();
+        dirty = false;
+    }
+    BatchView view(int kind, int block, cudaStream_t s)
+    {
+        sync(s);
+        auto key = std::make_pair(kind, block);
+        auto it = begins.find(key);
+        if (it == begins.end()) {
+            std::vector<int> b(lats.size() + 1, 0);
+            for (size_t i = 0; i < lats.size(); ++i)
+                b[i + 1] = b[i] + (work_of(lats[i]->desc, kind) + block - 1) / block;
+            auto buf = std::make_shared<DevBuf>();
+            buf->ensure(sizeof(int) * b.size());
+            ck(cudaMemcpyAsync(buf->p, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, s), "begin upload");
+            ck(cudaStreamSynchronize(s), "begin upload");
+            it = begins.emplace(key, std::make_pair(buf, b.back())).first;
+        }
+        BatchView v;
+        v.lats = reinterpret_cast<const LatDev*>(d_lats.p);
+        v.begin = reinterpret_cast<const int*>(it->second.first->p);
+        v.nlat = (int)lats.size();
+        v.nblocks = it->second.second;
+        return v;
+    }
+};
+
+#define OPS_CALL(N_, FN, ...)                                                      \
+    do {                                                                           \
+        cudaError_t e_;                                                            \
+        switch (N_) {                                                              \
+        case 2: e_ = Ops<2>::FN(__VA_ARGS__); break;                               \
+        case 3: e_ = Ops<3>::FN(__VA_ARGS__); break;                               \
+        case 4: e_ = Ops<4>::FN(__VA_ARGS__); break;                               \
+        case 6: e_ = Ops<6>::FN(__VA_ARGS__); break;                               \
+        default: fail(SUN_ERR_UNSUPPORTED, "N=%d not built", (int)(N_));          \
+        }                                                                          \
+        ck(e_, #FN);                                                               \
+    } while (0)
+
+// -- sweeps ------------------------------------------------------------------
+void group_sweep(sun_ctx* c, Group& g, int n_hb, int n_or, bool count_sweep, bool reunit, cudaStream_t s)
+{
+    if (g.lats.empty()) return;
+    BatchView half = g.view(WORK_HALF, c->blk_update, s);
+    InjView none{nullptr, 0, nullptr};
+    for (int h = 0; h < n_hb; ++h)
+        for (int par = 0; par < 2; ++par)
+            for (int mu = 0; mu < 4; ++mu)
+                OPS_CALL(g.N, update, g.fp64, g.layout, MODE_HB, half, c->blk_update, par, mu, (unsigned)h, none, s);
+    for (int o = 0; o < n_or; ++o)
+        for (int par = 0; par < 2; ++par)
+            for (int mu = 0; mu < 4; ++mu)
+                OPS_CALL(g.N, update, g.fp64, g.layout, MODE_OR, half, c->blk_update, par, mu, 0u, none, s);
+    if (n_hb > 0 || count_sweep)
+        ck(launch_end_sweep(reinterpret_cast<const LatDev*>(g.d_lats.p), (int)g.lats.size(), (unsigned)n_hb,
+                            count_sweep ? 1u : 0u, s),
+           "end_sweep");
+    // end_sweep above also bumped the sweep counter when count_sweep; the
+    // reunitarization kernel checks each lattice's own schedule on device
+    if (reunit) {
+        BatchView links = g.view(WORK_LINKS, c->blk_links, s);
+        OPS_CALL(g.N, reunit, g.fp64, g.layout, links, c->blk_links, 1, s);
+    }
+}
+
+bool group_needs_reunit(const Group& g)
+{
+    for (auto* l : g.lats)
+        if (l->p.reunit_every > 0) return true;
+    return false;
+}
+
+// -- measurements --------------------------------------------------------------
+// Runs a partial-producing kernel and the deterministic per-lattice finalize;
+// returns nvals doubles per lattice in g.h_out.
+template <class F> double* group_reduce(Group& g, int kind, int block, int nvals, bool is_max, cudaStream_t s, F launch)
+{
+    BatchView v = g.view(kind, block, s);
+    g.partials.ensure(sizeof(double) * 2 * (size_t)nvals * std::max(1, v.nblocks));
+    g.out.ensure(sizeof(double) * (size_t)nvals * g.lats.size());
+    g.h_out.ensure(sizeof(double) * (size_t)nvals * g.lats.size());
+    launch(v, reinterpret_cast<double*>(g.partials.p));
+    if (is_max)
+        ck(launch_finalize_max(v, reinterpret_cast<double*>(g.partials.p), reinterpret_cast<double*>(g.out.p), s),
+           "finalize");
+    else
+        ck(launch_finalize_sum(v, reinterpret_cast<double*>(g.partials.p), nvals, reinterpret_cast<double*>(g.out.p),
+                               s),
+           "finalize");
+    ck(cudaMemcpyAsync(g.h_out.p, g.out.p, sizeof(double) * nvals * g.lats.size(), cudaMemcpyDeviceToHost, s),
+       "result copy");
+    ck(cudaStreamSynchronize(s), "measurement");
+    return reinterpret_cast<double*>(g.h_out.p);
+}
+
+void group_plaquette(sun_ctx* c, Group& g, double* out, cudaStream_t s)
+{
+    double* r = group_reduce(g, WORK_SITES, c->blk_sites, 2, false, s, [&](const BatchView& v, double* part) {
+        OPS_CALL(g.N, plaquette, g.fp64, g.layout, v, c->blk_sites, part, s);
+    });
+    for (size_t i = 0; i < g.lats.size(); ++i) {
+        const LatDev& L = g.lats[i]->desc;
+        double norm = 3.0 * g.N * (double)L.V;
+        out[2 * i] = r[2 * i] / norm;
+        out[2 * i + 1] = r[2 * i + 1] / norm;
+    }
+}
+
+void group_polyakov(sun_ctx* c, Group& g, double* out, cudaStream_t s)
+{
+    double* r = group_reduce(g, WORK_SPATIAL, c->blk_sites, 2, false, s, [&](const BatchView& v, double* part) {
+        OPS_CALL(g.N, polyakov, g.fp64, g.layout, v, c->blk_sites, part, s);
+    });
+    for (size_t i = 0; i < g.lats.size(); ++i) {
+        const LatDev& L = g.lats[i]->desc;
+        double norm = (double)g.N * L.X[0] * L.X[1] * L.X[2];
+        out[2 * i] = r[2 * i] / norm;
+        out[2 * i + 1] = r[2 * i + 1] / norm;
+    }
+}
+
+// single-lattice group, cached in the lattice (tables and measurement
+// scratch persist across calls)
+struct Solo {
+    Group& g;
+    explicit Solo(sun_lattice* l) : g(*make(l)) {}
+    static Group* make(sun_lattice* l)
+    {
+        if (!l->solo) {
+            Group* g = new Group();
+            g->N = l->p.ncolors;
+            g->fp64 = l->p.precision == SUN_F64;
+            g->layout = l->p.layout;
+            g->lats.push_back(l);
+            l->solo = g;
+        }
+        return l->solo;
+    }
+};
+
+}  // namespace
+
+sun_lattice::~sun_lattice() { delete solo; }
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_err;  // errors without a context
+
+sun_status handle(sun_ctx* c, const std::function<void()>& f);
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Generic kernels (N-independent)
+namespace sunb {
+
+struct DDh { double s, c; };
+__device__ __forceinline__ DDh ddh_add(DDh a, DDh b)
+{
+    double s = a.s + b.s;
+    double bb = s - a.s;
+    double e = (a.s - (s - bb)) + (b.s - bb);
+    DDh r;
+    r.s = s;
+    r.c = (a.c + b.c) + e;
+    return r;
+}
+
+// one warp per lattice: lane-strided compensated sums over the lattice's
+// CTA partials, then a fixed shuffle tree -- identical result whatever else
+// shares the launch
+__global__ void k_finalize_sum(BatchView bv, const double* partials, int nvals, double* out)
+{
+    const int l = blockIdx.x;
+    const int lane = threadIdx.x;
+    const int b0 = bv.begin[l], b1 = bv.begin[l + 1];
+    for (int v = 0; v < nvals; ++v) {
+        DDh d{0.0, 0.0};
+        for (int b = b0 + lane; b < b1; b += 32) {
+            DDh t{partials[((size_t)b * nvals + v) * 2], partials[((size_t)b * nvals + v) * 2 + 1]};
+            d = ddh_add(d, t);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            DDh t{__shfl_down_sync(0xffffffffu, d.s, o), __shfl_down_sync(0xffffffffu, d.c, o)};
+            d = ddh_add(d, t);
+        }
+        if (lane == 0) out[(size_t)l * nvals + v] = d.s + d.c;
+    }
+}
+
+__global__ void k_finalize_max(BatchView bv, const double* partials, double* out)
+{
+    const int l = blockIdx.x;
+    const int lane = threadIdx.x;
+    double m = 0.0;
+    for (int b = bv.begin[l] + lane; b < bv.begin[l + 1]; b += 32) m = fmax(m, partials[(size_t)b * 2]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if (lane == 0) out[l] = m;
+}
+
+__global__ void k_end_sweep(const LatDev* lats, int nlat, unsigned n_hb, unsigned inc)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nlat) {
+        lats[i].state[0] += n_hb;
+        lats[i].state[1] += inc;
+    }
+}
+
+cudaError_t launch_finalize_sum(const BatchView& bv, const double* partials, int nvals, double* out, cudaStream_t s)
+{
+    k_finalize_sum<<<bv.nlat, 32, 0, s>>>(bv, partials, nvals, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_finalize_max(const BatchView& bv, const double* partials, double* out, cudaStream_t s)
+{
+    k_finalize_max<<<bv.nlat, 32, 0, s>>>(bv, partials, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_end_sweep(const LatDev* lats, int nlat, unsigned n_hb, unsigned inc, cudaStream_t s)
+{
+    k_end_sweep<<<(nlat + 127) / 128, 128, 0, s>>>(lats, nlat, n_hb, inc);
+    return cudaGetLastError();
+}
+
+}  // namespace sunb
+
+namespace {
+
+sun_status handle(sun_ctx* c, const std::function<void()>& f)
+{
+    try {
+        if (c) {
+            std::lock_guard<std::recursive_mutex> lk(c->mu);
+            f();
+        } else {
+            f();
+        }
+        return SUN_OK;
+    } catch (const Error& e) {
+        if (c) c->last_error = e.what();
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        g_err = e.what();
+        return e.st;
+    } catch (const std::bad_alloc&) {
+        if (c) c->last_error = "host allocation failed";
+        return SUN_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        if (c) c->last_error = e.what();
+        return SUN_ERR_CUDA;
+    }
+}
+
+void validate(const sun_lattice_params* p)
+{
+    if (!p) fail(SUN_ERR_INVALID_ARG, "null lattice parameters");
+    if (p->ncolors != 2 && p->ncolors != 3 && p->ncolors != 4 && p->ncolors != 6)
+        fail(SUN_ERR_UNSUPPORTED, "N=%d not supported (built: 2, 3, 4, 6)", p->ncolors);
+    for (int d = 0; d < 4; ++d) {
+        if (p->dims[d] < 2) fail(SUN_ERR_INVALID_ARG, "dimension %d = %d too small", d, p->dims[d]);
+        if (p->dims[d] % 2) fail(SUN_ERR_INVALID_ARG, "dimension %d = %d is odd (even/odd layout needs even)", d, p->dims[d]);
+    }
+    if (p->layout != SUN_SOA && p->layout != SUN_SOA12 && p->layout != SUN_SOA8)
+        fail(SUN_ERR_INVALID_ARG, "unknown layout %d", (int)p->layout);
+    if ((p->layout == SUN_SOA12 || p->layout == SUN_SOA8) && p->ncolors != 3)
+        fail(SUN_ERR_UNSUPPORTED, "12/8-parameter layouts exist for SU(3) only");
+    if (p->order != SUN_EVEN_ODD && p->order != SUN_NORMAL) fail(SUN_ERR_INVALID_ARG, "unknown order");
+    if (p->precision != SUN_F32 && p->precision != SUN_F64) fail(SUN_ERR_INVALID_ARG, "unknown precision");
+    if (p->reunit_every < 0) fail(SUN_ERR_INVALID_ARG, "reunit_every < 0");
+    double V = (double)p->dims[0] * p->dims[1] * p->dims[2] * p->dims[3];
+    double maxidx = V * 4.0 * elems_of(p->ncolors, p->layout);
+    if (maxidx >= 2147483647.0) fail(SUN_ERR_CAPACITY, "lattice too large for 32-bit element indexing");
+}
+
+void need_eo(sun_lattice* l, const char* what)
+{
+    if (l->p.order != SUN_EVEN_ODD)
+        fail(SUN_ERR_UNSUPPORTED, "%s needs an even/odd ordered array (as the reference kernels)", what);
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* sun_version(void) { return "sun_b200 0.1 (sm_100a)"; }
+
+const char* sun_last_error_string(const sun_ctx* c)
+{
+    if (c) return c->last_error.c_str();
+    return g_err.c_str();
+}
+
+sun_status sun_init(const sun_config* cfg, sun_ctx** out)
+{
+    return handle(nullptr, [&] {
+        if (!out) fail(SUN_ERR_INVALID_ARG, "null output");
+        auto c = std::make_unique<sun_ctx>();
+        c->device = cfg ? cfg->device : 0;
+        c->verbosity = cfg ? cfg->verbosity : 0;
+        int n = 0;
+        ck(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+        if (c->device < 0 || c->device >= n) fail(SUN_ERR_INVALID_ARG, "device %d not present (%d devices)", c->device, n);
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        c->err.ensure(sizeof(int));
+        ck(cudaMemset(c->err.p, 0, sizeof(int)), "memset");
+        size_t fr = 0, tot = 0;
+        ck(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+        c->hbm_budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (size_t)(0.9 * (double)fr);
+        *out = c.release();
+    });
+}
+
+sun_status sun_finalize(sun_ctx* c)
+{
+    if (!c) return SUN_ERR_INVALID_ARG;
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return SUN_OK;
+}
+
+sun_status sun_lattice_create(sun_ctx* c, const sun_lattice_params* p, sun_lattice** out)
+{
+    return handle(c, [&] {
+        if (!c || !out) fail(SUN_ERR_INVALID_ARG, "null argument");
+        validate(p);
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        auto l = std::make_unique<sun_lattice>();
+        l->ctx = c;
+        l->p = *p;
+        const int V = p->dims[0] * p->dims[1] * p->dims[2] * p->dims[3];
+        const size_t csz = p->precision == SUN_F64 ? 16 : 8;
+        l->bytes = csz * (size_t)elems_of(p->ncolors, p->layout) * 4 * (size_t)V;
+        l->links.ensure(l->bytes);
+        l->state.ensure(2 * sizeof(unsigned));
+        ck(cudaMemset(l->state.p, 0, 2 * sizeof(unsigned)), "memset");
+        ck(cudaMemset(l->links.p, 0, l->bytes), "memset");
+        LatDev& d = l->desc;
+        d.links = l->links.p;
+        for (int k = 0; k < 4; ++k) d.X[k] = p->dims[k];
+        d.V = V;
+        d.halfV = V / 2;
+        d.beta_over_n = p->beta / p->ncolors;
+        d.seed = p->seed;
+        d.state = reinterpret_cast<unsigned*>(l->state.p);
+        d.reunit_every = p->reunit_every;
+        d.evenodd = p->order == SUN_EVEN_ODD;
+        *out = l.release();
+    });
+}
+
+sun_status sun_lattice_destroy(sun_lattice* l)
+{
+    if (!l) return SUN_ERR_INVALID_ARG;
+    delete l;
+    return SUN_OK;
+}
+
+sun_status sun_lattice_bytes(const sun_lattice* l, size_t* b)
+{
+    if (!l || !b) return SUN_ERR_INVALID_ARG;
+    *b = l->bytes;
+    return SUN_OK;
+}
+
+sun_status sun_lattice_device_ptr(const sun_lattice* l, void** d)
+{
+    if (!l || !d) return SUN_ERR_INVALID_ARG;
+    *d = l->links.p;
+    return SUN_OK;
+}
+
+sun_status sun_lattice_init_cold(sun_lattice* l, void* stream)
+{
+    if (!l) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        // the 8-parameter form is singular at |a1| = 1 (gaugearray.cu:293-297)
+        if (l->p.layout == SUN_SOA8) fail(SUN_ERR_UNSUPPORTED, "SOA8 arrays cannot take a cold start");
+        cudaStream_t s = S(l->ctx, stream);
+        Solo so(l);
+        BatchView v = so.g.view(WORK_LINKS, l->ctx->blk_links, s);
+        OPS_CALL(l->p.ncolors, cold, so.g.fp64, so.g.layout, v, l->ctx->blk_links, s);
+        ck(cudaMemsetAsync(l->state.p, 0, 2 * sizeof(unsigned), s), "memset");
+        ck(cudaStreamSynchronize(s), "cold start");
+    });
+}
+
+sun_status sun_lattice_init_hot(sun_lattice* l, void* stream)
+{
+    if (!l) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        cudaStream_t s = S(l->ctx, stream);
+        Solo so(l);
+        BatchView v = so.g.view(WORK_SITES, 128, s);
+        OPS_CALL(l->p.ncolors, hot, so.g.fp64, so.g.layout, v, 128, s);
+        ck(cudaMemsetAsync(l->state.p, 0, 2 * sizeof(unsigned), s), "memset");
+        ck(cudaStreamSynchronize(s), "hot start");
+    });
+}
+
+static void canon_upload(sun_lattice* l, const void* host, cudaStream_t s, bool host_is_device)
+{
+    const size_t V = l->desc.V, N = l->p.ncolors;
+    const size_t bytes = V * 4 * N * N * 16;
+    DevBuf stage;
+    const void* src = host;
+    if (!host_is_device) {
+        stage.ensure(bytes);
+        ck(cudaMemcpyAsync(stage.p, host, bytes, cudaMemcpyHostToDevice, s), "upload");
+        src = stage.p;
+    }
+    Solo so(l);
+    BatchView v = so.g.view(WORK_LINKS, l->ctx->blk_links, s);
+    OPS_CALL(l->p.ncolors, pack, so.g.fp64, so.g.layout, v, l->ctx->blk_links, src, s);
+    ck(cudaStreamSynchronize(s), "upload");
+}
+
+static void canon_download(sun_lattice* l, void* host, cudaStream_t s)
+{
+    const size_t V = l->desc.V, N = l->p.ncolors;
+    const size_t bytes = V * 4 * N * N * 16;
+    DevBuf stage;
+    stage.ensure(bytes);
+    Solo so(l);
+    BatchView v = so.g.view(WORK_LINKS, l->ctx->blk_links, s);
+    OPS_CALL(l->p.ncolors, unpack, so.g.fp64, so.g.layout, v, l->ctx->blk_links, stage.p, s);
+    ck(cudaMemcpyAsync(host, stage.p, bytes, cudaMemcpyDeviceToHost, s), "download");
+    ck(cudaStreamSynchronize(s), "download");
+}
+
+sun_status sun_lattice_upload(sun_lattice* l, const void* host, sun_host_format fmt, void* stream)
+{
+    if (!l || !host) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        cudaStream_t s = S(l->ctx, stream);
+        if (fmt == SUN_HOST_IMAGE) {
+            ck(cudaMemcpyAsync(l->links.p, host, l->bytes, cudaMemcpyHostToDevice, s), "upload");
+            ck(cudaStreamSynchronize(s), "upload");
+        } else if (fmt == SUN_HOST_CANONICAL) {
+            canon_upload(l, host, s, false);
+        } else {
+            fail(SUN_ERR_INVALID_ARG, "unknown host format");
+        }
+    });
+}
+
+sun_status sun_lattice_download(sun_lattice* l, void* host, sun_host_format fmt, void* stream)
+{
+    if (!l || !host) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        cudaStream_t s = S(l->ctx, stream);
+        if (fmt == SUN_HOST_IMAGE) {
+            ck(cudaMemcpyAsync(host, l->links.p, l->bytes, cudaMemcpyDeviceToHost, s), "download");
+            ck(cudaStreamSynchronize(s), "download");
+        } else if (fmt == SUN_HOST_CANONICAL) {
+            canon_download(l, host, s);
+        } else {
+            fail(SUN_ERR_INVALID_ARG, "unknown host format");
+        }
+    });
+}
+
+sun_status sun_lattice_copy(sun_lattice* dst, sun_lattice* src, void* stream)
+{
+    if (!dst || !src) return SUN_ERR_INVALID_ARG;
+    return handle(dst->ctx, [&] {
+        if (dst->p.ncolors != src->p.ncolors) fail(SUN_ERR_INVALID_ARG, "copy between different N");
+        for (int k = 0; k < 4; ++k)
+            if (dst->p.dims[k] != src->p.dims[k]) fail(SUN_ERR_INVALID_ARG, "copy between different geometries");
+        cudaStream_t s = S(dst->ctx, stream);
+        const size_t V = src->desc.V, N = src->p.ncolors;
+        DevBuf stage;
+        stage.ensure(V * 4 * N * N * 16);
+        {
+            Solo so(src);
+            BatchView v = so.g.view(WORK_LINKS, src->ctx->blk_links, s);
+            OPS_CALL(src->p.ncolors, unpack, so.g.fp64, so.g.layout, v, src->ctx->blk_links, stage.p, s);
+        }
+        {
+            Solo so(dst);
+            BatchView v = so.g.view(WORK_LINKS, dst->ctx->blk_links, s);
+            OPS_CALL(dst->p.ncolors, pack, so.g.fp64, so.g.layout, v, dst->ctx->blk_links, stage.p, s);
+        }
+        ck(cudaMemcpyAsync(dst->state.p, src->state.p, 2 * sizeof(unsigned), cudaMemcpyDeviceToDevice, s), "copy");
+        ck(cudaStreamSynchronize(s), "copy");
+    });
+}
+
+sun_status sun_lattice_get_rng(sun_lattice* l, uint64_t* seed, uint32_t* hb, uint32_t* sw)
+{
+    if (!l) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        unsigned st[2];
+        ck(cudaMemcpy(st, l->state.p, sizeof st, cudaMemcpyDeviceToHost), "state read");
+        if (seed) *seed = l->p.seed;
+        if (hb) *hb = st[0];
+        if (sw) *sw = st[1];
+    });
+}
+
+sun_status sun_lattice_set_rng(sun_lattice* l, uint64_t seed, uint32_t hb, uint32_t sw)
+{
+    if (!l) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        unsigned st[2] = {hb, sw};
+        ck(cudaMemcpy(l->state.p, st, sizeof st, cudaMemcpyHostToDevice), "state write");
+        l->p.seed = seed;
+        l->desc.seed = seed;
+        ++l->version;
+    });
+}
+
+static void solo_passes(sun_lattice* l, int n_hb, int n_or, int n_sweeps, bool count, cudaStream_t s)
+{
+    need_eo(l, "the heatbath/overrelaxation update");
+    Solo so(l);
+    const bool re = count && l->p.reunit_every > 0;
+    for (int i = 0; i < n_sweeps; ++i) group_sweep(l->ctx, so.g, n_hb, n_or, count, re, s);
+}
+
+sun_status sun_heatbath(sun_lattice* l, int n, void* stream)
+{
+    if (!l || n < 0) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] { solo_passes(l, n, 0, 1, false, S(l->ctx, stream)); });
+}
+
+sun_status sun_overrelax(sun_lattice* l, int n, void* stream)
+{
+    if (!l || n < 0) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] { solo_passes(l, 0, n, 1, false, S(l->ctx, stream)); });
+}
+
+sun_status sun_sweep(sun_lattice* l, int n_hb, int n_or, int n_sweeps, void* stream)
+{
+    if (!l || n_hb < 0 || n_or < 0 || n_sweeps < 0) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] { solo_passes(l, n_hb, n_or, n_sweeps, true, S(l->ctx, stream)); });
+}
+
+sun_status sun_heatbath_injected(sun_lattice* l, const double* u, int stride, void* stream)
+{
+    if (!l || !u || stride <= 0) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        need_eo(l, "the heatbath update");
+        cudaStream_t s = S(l->ctx, stream);
+        Solo so(l);
+        BatchView half = so.g.view(WORK_HALF, l->ctx->blk_update, s);
+        ck(cudaMemsetAsync(l->ctx->err.p, 0, sizeof(int), s), "memset");
+        InjView inj{u, stride, reinterpret_cast<int*>(l->ctx->err.p)};
+        for (int par = 0; par < 2; ++par)
+            for (int mu = 0; mu < 4; ++mu)
+                OPS_CALL(l->p.ncolors, update, so.g.fp64, so.g.layout, MODE_HB_INJECTED, half, l->ctx->blk_update,
+                         par, mu, 0u, inj, s);
+        int flag = 0;
+        ck(cudaMemcpyAsync(&flag, l->ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "flag read");
+        ck(cudaStreamSynchronize(s), "heatbath");
+        if (flag) fail(SUN_ERR_DEVICE_FLAG, "injected uniform stream ran out (stride %d)", stride);
+    });
+}
+
+sun_status sun_reunitarize(sun_lattice* l, void* stream)
+{
+    if (!l) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        cudaStream_t s = S(l->ctx, stream);
+        Solo so(l);
+        BatchView v = so.g.view(WORK_LINKS, l->ctx->blk_links, s);
+        OPS_CALL(l->p.ncolors, reunit, so.g.fp64, so.g.layout, v, l->ctx->blk_links, 0, s);
+        ck(cudaStreamSynchronize(s), "reunitarize");
+    });
+}
+
+sun_status sun_unitarity_violation(sun_lattice* l, double* out, void* stream)
+{
+    if (!l || !out) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        cudaStream_t s = S(l->ctx, stream);
+        Solo so(l);
+        double* r = group_reduce(so.g, WORK_LINKS, 256, 1, true, s, [&](const BatchView& v, double* part) {
+            OPS_CALL(l->p.ncolors, unitarity, so.g.fp64, so.g.layout, v, 256, part, s);
+        });
+        *out = r[0];
+    });
+}
+
+sun_status sun_plaquette(sun_lattice* l, double out[2], void* stream)
+{
+    if (!l || !out) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        Solo so(l);
+        group_plaquette(l->ctx, so.g, out, S(l->ctx, stream));
+    });
+}
+
+sun_status sun_polyakov(sun_lattice* l, double out[2], void* stream)
+{
+    if (!l || !out) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        Solo so(l);
+        group_polyakov(l->ctx, so.g, out, S(l->ctx, stream));
+    });
+}
+
+sun_status sun_wilson_loops(sun_lattice* l, int R, int T, double* out, void* stream)
+{
+    if (!l || !out) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        if (R < 0 || T < 0 || R > 8 || T > 8) fail(SUN_ERR_INVALID_ARG, "Wilson loops need 0 <= R, T <= 8");
+        for (int d = 0; d < 3; ++d)
+            if (R >= l->p.dims[d]) fail(SUN_ERR_INVALID_ARG, "R=%d not below spatial extent %d", R, l->p.dims[d]);
+        if (T >= l->p.dims[3]) fail(SUN_ERR_INVALID_ARG, "T=%d not below temporal extent", T);
+        cudaStream_t s = S(l->ctx, stream);
+        Solo so(l);
+        const int nv = 2 * (R + 1) * (T + 1);
+        const int blk = l->ctx->blk_wilson;
+        double* r = group_reduce(so.g, WORK_SITES, blk, nv, false, s, [&](const BatchView& v, double* part) {
+            OPS_CALL(l->p.ncolors, wilson, so.g.fp64, so.g.layout, v, blk, R, T, part, s);
+        });
+        const double norm = 3.0 * l->p.ncolors * (double)l->desc.V;
+        for (int i = 0; i < nv; ++i) out[i] = r[i] / norm;
+    });
+}
+
+// gauge file: header int32 grid[4], beta (leading sizeof(Real) bytes of the
+// double), size_t sizeof(RealSave); body = canonical order in RealSave
+sun_status sun_save_bin(sun_lattice* l, const char* path, int save_fp64, int with_header)
+{
+    if (!l || !path) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        const size_t n = (size_t)l->desc.V * 4 * l->p.ncolors * l->p.ncolors * 2;
+        std::vector<double> buf(n);
+        canon_download(l, buf.data(), S(l->ctx, nullptr));
+        FILE* f = fopen(path, "wb");
+        if (!f) fail(SUN_ERR_IO, "cannot open %s for writing", path);
+        bool ok = true;
+        if (with_header) {
+            int g[4] = {l->p.dims[0], l->p.dims[1], l->p.dims[2], l->p.dims[3]};
+            ok &= fwrite(g, sizeof(int), 4, f) == 4;
+            double beta = l->p.beta;
+            ok &= fwrite(&beta, l->p.precision == SUN_F64 ? 8 : 4, 1, f) == 1;
+            size_t prec = save_fp64 ? 8 : 4;
+            ok &= fwrite(&prec, sizeof(size_t), 1, f) == 1;
+        }
+        if (save_fp64) {
+            ok &= fwrite(buf.data(), sizeof(double), n, f) == n;
+        } else {
+            std::vector<float> t(n);
+            for (size_t i = 0; i < n; ++i) t[i] = (float)buf[i];
+            ok &= fwrite(t.data(), sizeof(float), n, f) == n;
+        }
+        ok &= fclose(f) == 0;
+        if (!ok) fail(SUN_ERR_IO, "write to %s failed", path);
+    });
+}
+
+sun_status sun_load_bin(sun_lattice* l, const char* path, int save_fp64, int with_header)
+{
+    if (!l || !path) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        const size_t n = (size_t)l->desc.V * 4 * l->p.ncolors * l->p.ncolors * 2;
+        FILE* f = fopen(path, "rb");
+        if (!f) fail(SUN_ERR_IO, "cannot open %s", path);
+        std::unique_ptr<FILE, int (*)(FILE*)> guard(f, fclose);
+        if (with_header) {
+            int g[4];
+            if (fread(g, sizeof(int), 4, f) != 4) fail(SUN_ERR_IO, "%s: short header", path);
+            for (int k = 0; k < 4; ++k)
+                if (g[k] != l->p.dims[k]) fail(SUN_ERR_INVALID_ARG, "%s: grid mismatch (%d vs %d in dim %d)", path, g[k], l->p.dims[k], k);
+            double beta = 0;
+            if (fread(&beta, l->p.precision == SUN_F64 ? 8 : 4, 1, f) != 1) fail(SUN_ERR_IO, "%s: short header", path);
+            size_t prec = 0;
+            if (fread(&prec, sizeof(size_t), 1, f) != 1) fail(SUN_ERR_IO, "%s: short header", path);
+            if (prec != (size_t)(save_fp64 ? 8 : 4))
+                fail(SUN_ERR_INVALID_ARG, "%s: stored precision %zu does not match %d", path, prec, save_fp64 ? 8 : 4);
+        }
+        std::vector<double> buf(n);
+        if (save_fp64) {
+            if (fread(buf.data(), sizeof(double), n, f) != n) fail(SUN_ERR_IO, "%s: truncated body", path);
+        } else {
+            std::vector<float> t(n);
+            if (fread(t.data(), sizeof(float), n, f) != n) fail(SUN_ERR_IO, "%s: truncated body", path);
+            for (size_t i = 0; i < n; ++i) buf[i] = t[i];
+        }
+        canon_upload(l, buf.data(), S(l->ctx, nullptr), false);
+    });
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batches
+struct sun_batch {
+    sun_ctx* ctx = nullptr;
+    std::vector<sun_lattice*> order;        // insertion order
+    std::vector<std::unique_ptr<Group>> groups;
+    cudaGraphExec_t graph = nullptr;
+    int graph_hb = -1, graph_or = -1;
+    bool dirty = true;
+
+    ~sun_batch() { drop_graph(); }
+    void drop_graph()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
+    void regroup()
+    {
+        if (!dirty) return;
+        groups.clear();
+        for (auto* l : order) {
+            int fp64 = l->p.precision == SUN_F64, lay = l->p.layout;
+            Group* g = nullptr;
+            for (auto& gg : groups)
+                if (gg->N == l->p.ncolors && gg->fp64 == fp64 && gg->layout == lay) g = gg.get();
+            if (!g) {
+                groups.emplace_back(new Group());
+                g = groups.back().get();
+                g->N = l->p.ncolors;
+                g->fp64 = fp64;
+                g->layout = lay;
+            }
+            g->lats.push_back(l);
+        }
+        drop_graph();
+        dirty = false;
+    }
+};
+
+namespace {
+
+void batch_one_sweep(sun_batch* b, int n_hb, int n_or, cudaStream_t s)
+{
+    for (auto& g : b->groups) group_sweep(b->ctx, *g, n_hb, n_or, true, group_needs_reunit(*g), s);
+}
+
+}  // namespace
+
+extern "C" {
+
+sun_status sun_batch_create(sun_ctx* c, sun_batch** out)
+{
+    return handle(c, [&] {
+        if (!c || !out) fail(SUN_ERR_INVALID_ARG, "null argument");
+        auto b = std::make_unique<sun_batch>();
+        b->ctx = c;
+        *out = b.release();
+    });
+}
+
+sun_status sun_batch_destroy(sun_batch* b)
+{
+    if (!b) return SUN_ERR_INVALID_ARG;
+    delete b;
+    return SUN_OK;
+}
+
+sun_status sun_batch_add(sun_batch* b, sun_lattice* l)
+{
+    if (!b || !l) return SUN_ERR_INVALID_ARG;
+    return handle(b->ctx, [&] {
+        need_eo(l, "batched sweeps");
+        if (std::find(b->order.begin(), b->order.end(), l) != b->order.end())
+            fail(SUN_ERR_INVALID_ARG, "lattice already in batch");
+        b->order.push_back(l);
+        b->dirty = true;
+    });
+}
+
+sun_status sun_batch_remove(sun_batch* b, sun_lattice* l)
+{
+    if (!b || !l) return SUN_ERR_INVALID_ARG;
+    return handle(b->ctx, [&] {
+        auto it = std::find(b->order.begin(), b->order.end(), l);
+        if (it == b->order.end()) fail(SUN_ERR_INVALID_ARG, "lattice not in batch");
+        b->order.erase(it);
+        b->dirty = true;
+    });
+}
+
+sun_status sun_batch_size(const sun_batch* b, int* n)
+{
+    if (!b || !n) return SUN_ERR_INVALID_ARG;
+    *n = (int)b->order.size();
+    return SUN_OK;
+}
+
+sun_status sun_batch_sweep(sun_batch* b, int n_hb, int n_or, int n_sweeps, int use_graph, void* stream)
+{
+    if (!b || n_hb < 0 || n_or < 0 || n_sweeps < 0) return SUN_ERR_INVALID_ARG;
+    return handle(b->ctx, [&] {
+        b->regroup();
+        cudaStream_t s = S(b->ctx, stream);
+        if (b->order.empty() || n_sweeps == 0) return;
+        if (!use_graph) {
+            for (int i = 0; i < n_sweeps; ++i) batch_one_sweep(b, n_hb, n_or, s);
+            ck(cudaStreamSynchronize(s), "batch sweep");
+            return;
+        }
+        if (!b->graph || b->graph_hb != n_hb || b->graph_or != n_or) {
+            b->drop_graph();
+            // tables must exist before capture (their uploads synchronise)
+            for (auto& g : b->groups) {
+                g->view(WORK_HALF, b->ctx->blk_update, s);
+                g->view(WORK_LINKS, b->ctx->blk_links, s);
+            }
+            cudaStream_t cs;
+            ck(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+            cudaGraph_t graph;
+            ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "capture");
+            try {
+                batch_one_sweep(b, n_hb, n_or, cs);
+            } catch (...) {
+                cudaStreamEndCapture(cs, &graph);
+                cudaStreamDestroy(cs);
+                throw;
+            }
+            ck(cudaStreamEndCapture(cs, &graph), "capture end");
+            cudaStreamDestroy(cs);
+            cudaError_t e = cudaGraphInstantiate(&b->graph, graph, 0);
+            cudaGraphDestroy(graph);
+            ck(e, "graph instantiate");
+            b->graph_hb = n_hb;
+            b->graph_or = n_or;
+        }
+        for (int i = 0; i < n_sweeps; ++i) ck(cudaGraphLaunch(b->graph, s), "graph launch");
+        ck(cudaStreamSynchronize(s), "batch sweep");
+    });
+}
+
+static sun_status batch_measure(sun_batch* b, double* out, void* stream, bool plaq)
+{
+    if (!b || !out) return SUN_ERR_INVALID_ARG;
+    return handle(b->ctx, [&] {
+        b->regroup();
+        cudaStream_t s = S(b->ctx, stream);
+        for (auto& g : b->groups) {
+            std::vector<double> r(2 * g->lats.size());
+            if (plaq) group_plaquette(b->ctx, *g, r.data(), s);
+            else group_polyakov(b->ctx, *g, r.data(), s);
+            for (size_t i = 0; i < g->lats.size(); ++i) {
+                size_t pos = std::find(b->order.begin(), b->order.end(), g->lats[i]) - b->order.begin();
+                out[2 * pos] = r[2 * i];
+                out[2 * pos + 1] = r[2 * i + 1];
+            }
+        }
+    });
+}
+
+sun_status sun_batch_plaquette(sun_batch* b, double* out, void* stream) { return batch_measure(b, out, stream, true); }
+sun_status sun_batch_polyakov(sun_batch* b, double* out, void* stream) { return batch_measure(b, out, stream, false); }
+
+}  // extern "C"

@@ -1,0 +1,667 @@
+// sun_kernels.cuh -- the sm_100a kernels of the engine and the host launch
+// wrappers Ops<N>.  Included only by ops_n{2,3,4,6}.cu, one translation unit
+// per colour number N.
+//
+// Every launch covers a table of lattices of one (N, precision, layout)
+// class; CTA b finds its lattice by a binary search over the table's CTA
+// prefix (BatchView::begin), so one launch advances many uneven lattices.
+#pragma once
+#include "sun_core.cuh"
+#include "sun_ops.h"
+
+namespace sunb {
+
+SUN_DEV int find_lat(const BatchView& bv, int b)
+{
+    int lo = 0, hi = bv.nlat - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(bv.begin + mid) <= b) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+SUN_DEV Geom geom_of(const LatDev& L)
+{
+    Geom g;
+    g.X[0] = L.X[0]; g.X[1] = L.X[1]; g.X[2] = L.X[2]; g.X[3] = L.X[3];
+    g.V = L.V; g.halfV = L.halfV;
+    return g;
+}
+
+// y = x shifted by s (+1/-1) along direction d (d may be a runtime value)
+SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
+{
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int v = x[k] + (k == d ? s : 0);
+        v = v < 0 ? v + g.X[k] : (v >= g.X[k] ? v - g.X[k] : v);
+        y[k] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Checkerboard update of the links (x, mu) with parity(x) == parity --
+// kernel_PHeatBath_evenodd (src/monte/monte.cu:44-88) and
+// kernel_overrelaxation_evenodd (src/monte/ovr.cu:41-80).  One thread per
+// half-lattice site; the staple sum keeps the reference's order (nu ascending,
+// "up" then "down"); neighbour links are read through the read-only path
+// (they are never written in this phase), the own link through plain loads.
+template <int N, class R, int LAYOUT, int MODE>
+__global__ void __launch_bounds__(128) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
+                                                InjView inj)
+{
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int id = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    if (id >= g.halfV) return;
+    typedef LinkIO<N, R, LAYOUT> IO;
+    const cx<R>* base = reinterpret_cast<const cx<R>*>(L.links);
+    const uint32_t V = (uint32_t)g.V, stride = 4u * V;
+
+    int x[4];
+    eo_coords(g, id, parity, x);
+    const int sx = id + parity * g.halfV;
+    int xpmu[4];
+    shifted(g, x, mu, 1, xpmu);
+    const int sxpmu = eo_of(g, xpmu);
+
+    Mat<N, R> S;
+    mzero(S);
+#pragma unroll
+    for (int nu = 0; nu < 4; ++nu) {
+        if (nu == mu) continue;
+        int y[4];
+        Mat<N, R> A, B, C;
+        // up: U_nu(x) U_mu(x+nu) U_nu(x+mu)^dagger
+        shifted(g, x, nu, 1, y);
+        IO::template load<true>(base, sx + nu * V, stride, A);
+        IO::template load<true>(base, eo_of(g, y) + mu * V, stride, B);
+        mmul(A, B, C);
+        IO::template load<true>(base, sxpmu + nu * V, stride, A);
+        macc_nd(C, A, S);
+        // down: U_nu(x-nu)^dagger U_mu(x-nu) U_nu(x-nu+mu)
+        shifted(g, x, nu, -1, y);
+        const int sy = eo_of(g, y);
+        IO::template load<true>(base, sy + nu * V, stride, A);
+        IO::template load<true>(base, sy + mu * V, stride, B);
+        mmul_dn(A, B, C);
+        int z[4];
+        shifted(g, y, mu, 1, z);
+        IO::template load<true>(base, eo_of(g, z) + nu * V, stride, A);
+        macc(C, A, S);
+    }
+
+    cx<R>* wbase = reinterpret_cast<cx<R>*>(L.links);
+    const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
+    Mat<N, R> U;
+    IO::template load<false>(wbase, own, stride, U);
+    if constexpr (MODE == MODE_OR) {
+        overrelax_update<N, R>(U, S);
+    } else {
+        const int lex = lex_of(g, x);
+        const R bon = (R)L.beta_over_n;
+        if constexpr (MODE == MODE_HB) {
+            PhiloxStream<R> st;
+            st.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
+            heatbath_update<N, R>(U, S, bon, st);
+        } else {
+            InjectedStream<R> st;
+            st.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
+            st.left = inj.stride;
+            st.err = inj.err;
+            heatbath_update<N, R>(U, S, bon, st);
+        }
+    }
+    IO::store(wbase, own, stride, U);
+}
+
+// ---------------------------------------------------------------------------
+// Link-wise kernels: work index w over 4V links, w = site * 4 + mu with
+// `site` in the lattice's storage order.
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(256) k_cold(BatchView bv)
+{
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    if (w >= 4 * L.V) return;
+    Mat<N, R> U;
+    munit(U);
+    LinkIO<N, R, LAYOUT>::store(reinterpret_cast<cx<R>*>(L.links), (uint32_t)w, 4u * L.V, U);
+}
+
+// Haar-random SU(N) link (a new definition; the reference's hot start,
+// gaugearray.cu:355, is uniform entries + reunitarization, not Haar): a
+// complex Gaussian matrix from Philox stream (lex, mu | 1 << 8, pass 0) --
+// entry (i,j) by Box-Muller on FP64 uniforms u1, u2 -- then modified
+// Gram-Schmidt over columns (QR with positive diagonal) and the phase
+// exp(-i arg(det)/N) onto SU(N).  Computed in FP64, stored in R.
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(128) k_hot(BatchView bv)
+{
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int s = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    if (s >= g.V) return;
+    int x[4];
+    int site;
+    if (L.evenodd) {
+        const int par = s >= g.halfV;
+        eo_coords(g, s - par * g.halfV, par, x);
+        site = s;
+    } else {
+        lex_coords(g, s, x);
+        site = s;
+    }
+    const int lex = lex_of(g, x);
+    for (int mu = 0; mu < 4; ++mu) {
+        PhiloxStream<double> st;
+        st.init(L.seed, (uint32_t)lex, (uint32_t)mu | (1u << 8), 0u);
+        Mat<N, double> Q;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                double u1 = st.uniform();
+                double u2 = st.uniform();
+                double rad = sqrt(-2.0 * log(u1));
+                double sn, cs;
+                sincospi(2.0 * u2, &sn, &cs);
+                Q.e[i][j] = mkc(rad * cs, rad * sn);
+            }
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+#pragma unroll
+            for (int i = 0; i < j; ++i) {
+                cx<double> d = mkc(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < N; ++c) d = cfma_cn(Q.e[c][i], Q.e[c][j], d);
+#pragma unroll
+                for (int c = 0; c < N; ++c) Q.e[c][j] = Q.e[c][j] - d * Q.e[c][i];
+            }
+            double n = 0.0;
+#pragma unroll
+            for (int c = 0; c < N; ++c) n += cnorm2(Q.e[c][j]);
+            n = 1.0 / sqrt(n);
+#pragma unroll
+            for (int c = 0; c < N; ++c) Q.e[c][j] = n * Q.e[c][j];
+        }
+        cx<double> d = mdet<N, double>(Q);
+        double ph = atan2(d.im, d.re) / N;
+        double sn, cs;
+        sincos(ph, &sn, &cs);
+        const cx<double> f = mkc(cs, -sn);
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int j = 0; j < N; ++j) Q.e[i][j] = Q.e[i][j] * f;
+        Mat<N, R> U;
+        mconvert(Q, U);
+        LinkIO<N, R, LAYOUT>::store(reinterpret_cast<cx<R>*>(L.links), (uint32_t)site + (uint32_t)mu * g.V,
+                                    4u * g.V, U);
+    }
+}
+
+// FP64 reunitarization of every link -- kernel_calc_reunitarize
+// (src/reunitarize.cu:23-31), always in double arithmetic.
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(256) k_reunit(BatchView bv, int only_due)
+{
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    if (only_due) {
+        if (L.reunit_every <= 0) return;
+        const unsigned sw = L.state[1];
+        if (sw == 0u || (sw % (unsigned)L.reunit_every) != 0u) return;
+    }
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    if (w >= 4 * L.V) return;
+    cx<R>* base = reinterpret_cast<cx<R>*>(L.links);
+    Mat<N, R> U;
+    LinkIO<N, R, LAYOUT>::template load<false>(base, (uint32_t)w, 4u * L.V, U);
+    Mat<N, double> D;
+    mconvert(U, D);
+    reunit<N, double>(D);
+    mconvert(D, U);
+    LinkIO<N, R, LAYOUT>::store(base, (uint32_t)w, 4u * L.V, U);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic FP64 reductions: Neumaier/TwoSum-compensated pairs, reduced
+// in a fixed tree (warp shuffles, then one warp over the warp results).
+struct DD { double s, c; };
+SUN_DEV DD dd_add(DD a, DD b)
+{
+    double s = a.s + b.s;
+    double bb = s - a.s;
+    double e = (a.s - (s - bb)) + (b.s - bb);
+    DD r;
+    r.s = s;
+    r.c = (a.c + b.c) + e;
+    return r;
+}
+SUN_DEV DD dd_warp(DD d)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        DD t;
+        t.s = __shfl_down_sync(0xffffffffu, d.s, o);
+        t.c = __shfl_down_sync(0xffffffffu, d.c, o);
+        d = dd_add(d, t);
+    }
+    return d;
+}
+// reduces v over the CTA; thread 0 writes (sum, comp) to out[0..1]
+SUN_DEV void block_sum(double v, double* out, DD* sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    DD d;
+    d.s = v; d.c = 0.0;
+    d = dd_warp(d);
+    if (lane == 0) sh[warp] = d;
+    __syncthreads();
+    if (warp == 0) {
+        DD t;
+        if (lane < nw) t = sh[lane]; else { t.s = 0.0; t.c = 0.0; }
+        t = dd_warp(t);
+        if (lane == 0) { out[0] = t.s; out[1] = t.c; }
+    }
+    __syncthreads();
+}
+SUN_DEV void block_max(double v, double* out, double* sh)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        double t = lane < nw ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_down_sync(0xffffffffu, t, o));
+        if (lane == 0) { out[0] = t; out[1] = 0.0; }
+    }
+    __syncthreads();
+}
+
+// site w of a sites-launch -> coordinates (storage order of the lattice)
+SUN_DEV void site_coords(const LatDev& L, const Geom& g, int w, int x[4])
+{
+    if (L.evenodd) {
+        const int par = w >= g.halfV;
+        eo_coords(g, w - par * g.halfV, par, x);
+    } else {
+        lex_coords(g, w, x);
+    }
+}
+SUN_DEV int site_index(const LatDev& L, const Geom& g, const int x[4])
+{
+    return L.evenodd ? eo_of(g, x) : lex_of(g, x);
+}
+
+template <int N, class R, int LAYOUT>
+SUN_DEV void load_d(const LatDev& L, const Geom& g, const int x[4], int mu, Mat<N, double>& D)
+{
+    Mat<N, R> A;
+    LinkIO<N, R, LAYOUT>::template load<true>(reinterpret_cast<const cx<R>*>(L.links),
+                                              (uint32_t)site_index(L, g, x) + (uint32_t)mu * g.V,
+                                              4u * g.V, A);
+    mconvert(A, D);
+}
+
+// Plaquette -- kernel_calc_plaquette_evenodd_cub / _normal_cub
+// (src/meas/plaquette_cub.cu:47-145): per site sum over mu < nu of
+// Re tr[U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag], nu == 3 temporal.
+// Links are widened to FP64 before the products.
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partials)
+{
+    __shared__ DD sh[32];
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    double sp = 0.0, tp = 0.0;
+    if (w < g.V) {
+        int x[4];
+        site_coords(L, g, w, x);
+#pragma unroll 1
+        for (int mu = 0; mu < 3; ++mu) {
+            int xm[4];
+            shifted(g, x, mu, 1, xm);
+#pragma unroll 1
+            for (int nu = mu + 1; nu < 4; ++nu) {
+                int xn[4];
+                shifted(g, x, nu, 1, xn);
+                Mat<N, double> A, B, P, Q;
+                load_d<N, R, LAYOUT>(L, g, x, mu, A);
+                load_d<N, R, LAYOUT>(L, g, xm, nu, B);
+                mmul(A, B, P);
+                load_d<N, R, LAYOUT>(L, g, x, nu, A);
+                load_d<N, R, LAYOUT>(L, g, xn, mu, B);
+                mmul(A, B, Q);
+                const double t = mtrace_nd(P, Q).re;
+                if (nu == 3) tp += t; else sp += t;
+            }
+        }
+    }
+    block_sum(sp, partials + (size_t)b * 4, sh);
+    block_sum(tp, partials + (size_t)b * 4 + 2, sh);
+}
+
+// Polyakov loop -- kernel_calc_polyakovloop_evenodd
+// (src/meas/polyakovloop.cu:54-96): one thread per spatial site,
+// L = U_3(x,0) U_3(x,1) ... U_3(x,T-1), trace summed.
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials)
+{
+    __shared__ DD sh[32];
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int V3 = g.X[0] * g.X[1] * g.X[2];
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    double re = 0.0, im = 0.0;
+    if (w < V3) {
+        int x[4];
+        x[0] = w % g.X[0];
+        x[1] = (w / g.X[0]) % g.X[1];
+        x[2] = w / (g.X[0] * g.X[1]);
+        x[3] = 0;
+        Mat<N, double> P, A, T;
+        munit(P);
+#pragma unroll 1
+        for (int t = 0; t < g.X[3]; ++t) {
+            x[3] = t;
+            load_d<N, R, LAYOUT>(L, g, x, 3, A);
+            mmul(P, A, T);
+            P = T;
+        }
+        const cx<double> tr = mtrace(P);
+        re = tr.re;
+        im = tr.im;
+    }
+    block_sum(re, partials + (size_t)b * 4, sh);
+    block_sum(im, partials + (size_t)b * 4 + 2, sh);
+}
+
+// Planar Wilson loops W(r,t), r <= R, t <= T, averaged over the 3 spatial
+// directions -- kernel_WilsonLineSP + kernel_WilsonLoopSP
+// (src/meas/wilsonloop.cu:60-128), without the V*3*R temporary of spatial
+// lines: each thread keeps the T+1 spatial lines of its site in local
+// memory and builds the temporal lines on the fly.
+#define SUN_WMAX 8
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(64) k_wilson(BatchView bv, int RR, int TT, double* partials)
+{
+    __shared__ DD sh[32];
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    const int nres = (RR + 1) * (TT + 1);
+    double acc[2 * (SUN_WMAX + 1) * (SUN_WMAX + 1)];
+    for (int i = 0; i < 2 * nres; ++i) acc[i] = 0.0;
+    if (w < g.V) {
+        int x[4];
+        site_coords(L, g, w, x);
+        Mat<N, double> Ls[SUN_WMAX + 1];
+#pragma unroll 1
+        for (int mu = 0; mu < 3; ++mu) {
+#pragma unroll 1
+            for (int t = 0; t <= TT; ++t) munit(Ls[t]);
+#pragma unroll 1
+            for (int r = 0; r <= RR; ++r) {
+                if (r > 0) {
+#pragma unroll 1
+                    for (int t = 0; t <= TT; ++t) {
+                        int y[4] = {x[0], x[1], x[2], x[3]};
+                        y[3] = (x[3] + t) % g.X[3];
+                        int c = y[0] * (mu == 0) + y[1] * (mu == 1) + y[2] * (mu == 2);
+                        c = (c + r - 1) % g.X[mu];
+                        if (mu == 0) y[0] = c; else if (mu == 1) y[1] = c; else y[2] = c;
+                        Mat<N, double> A, T2;
+                        load_d<N, R, LAYOUT>(L, g, y, mu, A);
+                        mmul(Ls[t], A, T2);
+                        Ls[t] = T2;
+                    }
+                }
+                int xr[4] = {x[0], x[1], x[2], x[3]};
+                {
+                    int c = x[0] * (mu == 0) + x[1] * (mu == 1) + x[2] * (mu == 2);
+                    c = (c + r) % g.X[mu];
+                    if (mu == 0) xr[0] = c; else if (mu == 1) xr[1] = c; else xr[2] = c;
+                }
+                Mat<N, double> T0, T1, P, Q, A;
+                munit(T0);
+                munit(T1);
+#pragma unroll 1
+                for (int t = 0; t <= TT; ++t) {
+                    // tr[L0 T1 Lt^dag T0^dag] = sum_ij (L0 T1)_ij conj((T0 Lt)_ij)
+                    mmul(Ls[0], T1, P);
+                    mmul(T0, Ls[t], Q);
+                    const cx<double> wv = mtrace_nd(P, Q);
+                    acc[2 * (t + r * (TT + 1))] += wv.re;
+                    acc[2 * (t + r * (TT + 1)) + 1] += wv.im;
+                    if (t < TT) {
+                        int y[4] = {x[0], x[1], x[2], (x[3] + t) % g.X[3]};
+                        load_d<N, R, LAYOUT>(L, g, y, 3, A);
+                        mmul(T0, A, P);
+                        T0 = P;
+                        int z[4] = {xr[0], xr[1], xr[2], (x[3] + t) % g.X[3]};
+                        load_d<N, R, LAYOUT>(L, g, z, 3, A);
+                        mmul(T1, A, P);
+                        T1 = P;
+                    }
+                }
+            }
+        }
+    }
+    for (int i = 0; i < 2 * nres; ++i) block_sum(acc[i], partials + ((size_t)b * 2 * nres + i) * 2, sh);
+}
+
+// max over links of max_ij |(U^dag U - 1)_ij| (FP64)
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(256) k_unitarity(BatchView bv, double* partials)
+{
+    __shared__ double sh[32];
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    double worst = 0.0;
+    if (w < 4 * L.V) {
+        Mat<N, R> A;
+        LinkIO<N, R, LAYOUT>::template load<true>(reinterpret_cast<const cx<R>*>(L.links), (uint32_t)w,
+                                                  4u * L.V, A);
+        Mat<N, double> D, P;
+        mconvert(A, D);
+        mmul_dn(D, D, P);
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                cx<double> e = P.e[i][j];
+                if (i == j) e.re -= 1.0;
+                worst = fmax(worst, sqrt(cnorm2(e)));
+            }
+    }
+    block_max(worst, partials + (size_t)b * 2, sh);
+}
+
+// canonical FP64 (site lex, mu, N*N row-major) <-> device image; work over
+// 4V links with w = lex*4 + mu
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(256) k_pack(BatchView bv, const double2* canon)
+{
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    if (w >= 4 * g.V) return;
+    const int lex = w >> 2, mu = w & 3;
+    int x[4];
+    lex_coords(g, lex, x);
+    Mat<N, R> U;
+    const double2* src = canon + (size_t)w * N * N;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            double2 v = src[i * N + j];
+            U.e[i][j] = mkc<R>((R)v.x, (R)v.y);
+        }
+    LinkIO<N, R, LAYOUT>::store(reinterpret_cast<cx<R>*>(L.links),
+                                (uint32_t)site_index(L, g, x) + (uint32_t)mu * g.V, 4u * g.V, U);
+}
+
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(256) k_unpack(BatchView bv, double2* canon)
+{
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    if (w >= 4 * g.V) return;
+    const int lex = w >> 2, mu = w & 3;
+    int x[4];
+    lex_coords(g, lex, x);
+    Mat<N, R> U;
+    LinkIO<N, R, LAYOUT>::template load<false>(reinterpret_cast<const cx<R>*>(L.links),
+                                               (uint32_t)site_index(L, g, x) + (uint32_t)mu * g.V,
+                                               4u * g.V, U);
+    double2* dst = canon + (size_t)w * N * N;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) dst[i * N + j] = make_double2((double)U.e[i][j].re, (double)U.e[i][j].im);
+}
+
+// ---------------------------------------------------------------------------
+// Host launch wrappers: runtime (precision, layout) -> template instance.
+// SOA12 and SOA8 exist for N == 3 only (the reference silently falls back to
+// SOA for other N, gaugearray.h:127-137; the C ABI rejects them instead).
+#define SUN_DISPATCH(FP64, LAYOUT, CALL)                                            \
+    do {                                                                            \
+        if constexpr (N == 3) {                                                     \
+            if ((LAYOUT) == L_SOA12) {                                              \
+                if (FP64) { CALL(double, L_SOA12); } else { CALL(float, L_SOA12); } \
+            } else if ((LAYOUT) == L_SOA8) {                                        \
+                if (FP64) { CALL(double, L_SOA8); } else { CALL(float, L_SOA8); }   \
+            } else {                                                                \
+                if (FP64) { CALL(double, L_SOA); } else { CALL(float, L_SOA); }     \
+            }                                                                       \
+        } else {                                                                    \
+            if (FP64) { CALL(double, L_SOA); } else { CALL(float, L_SOA); }         \
+        }                                                                           \
+    } while (0)
+
+template <int N>
+cudaError_t Ops<N>::update(int fp64, int layout, int mode, const BatchView& bv, int block, int parity, int mu,
+                           unsigned hb_offset, const InjView& inj, cudaStream_t s)
+{
+#define CALL(R_, L_)                                                                                   \
+    if (mode == MODE_OR) k_update<N, R_, L_, MODE_OR><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
+    else if (mode == MODE_HB) k_update<N, R_, L_, MODE_HB><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
+    else k_update<N, R_, L_, MODE_HB_INJECTED><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N> cudaError_t Ops<N>::cold(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s)
+{
+#define CALL(R_, L_) k_cold<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N> cudaError_t Ops<N>::hot(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s)
+{
+#define CALL(R_, L_) k_hot<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::reunit(int fp64, int layout, const BatchView& bv, int block, int only_due, cudaStream_t s)
+{
+#define CALL(R_, L_) k_reunit<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, only_due)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::plaquette(int fp64, int layout, const BatchView& bv, int block, double* partials,
+                              cudaStream_t s)
+{
+#define CALL(R_, L_) k_plaquette<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::polyakov(int fp64, int layout, const BatchView& bv, int block, double* partials,
+                             cudaStream_t s)
+{
+#define CALL(R_, L_) k_polyakov<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::wilson(int fp64, int layout, const BatchView& bv, int block, int R, int T, double* partials,
+                           cudaStream_t s)
+{
+#define CALL(R_, L_) k_wilson<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, R, T, partials)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::unitarity(int fp64, int layout, const BatchView& bv, int block, double* partials,
+                              cudaStream_t s)
+{
+#define CALL(R_, L_) k_unitarity<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::pack(int fp64, int layout, const BatchView& bv, int block, const void* canon, cudaStream_t s)
+{
+#define CALL(R_, L_) k_pack<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, reinterpret_cast<const double2*>(canon))
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::unpack(int fp64, int layout, const BatchView& bv, int block, void* canon, cudaStream_t s)
+{
+#define CALL(R_, L_) k_unpack<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, reinterpret_cast<double2*>(canon))
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+}  // namespace sunb

@@ -1,0 +1,83 @@
+// sun_ops.h -- host-side launch interface between the C-ABI engine
+// (engine.cu) and the per-N kernel translation units (ops_n*.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sunb {
+
+// One lattice as every kernel sees it (an entry of a device table).
+struct LatDev {
+    void* links;              // device image, layout/precision of the class
+    int X[4];
+    int V, halfV;
+    double beta_over_n;       // beta / N (constants.cu:443)
+    unsigned long long seed;  // Philox key
+    unsigned int* state;      // device counters: [0] heatbath passes, [1] sweeps
+    int reunit_every;         // reunitarize when sweeps % reunit_every == 0 (0: never)
+    int evenodd;              // storage order: 1 even/odd, 0 lexicographic
+};
+
+// A launch over several lattices of one class (same N, precision, layout):
+// CTA b works on lattice l with begin[l] <= b < begin[l+1].
+struct BatchView {
+    const LatDev* lats;
+    const int* begin;
+    int nlat;
+    int nblocks;
+};
+
+// Uniforms injected per link for oracle parity: link (lex, mu) reads
+// u[(lex*4 + mu)*stride + k], k < stride.
+struct InjView {
+    const double* u;
+    int stride;
+    int* err;
+};
+
+enum UpdateMode { MODE_HB = 0, MODE_HB_INJECTED = 1, MODE_OR = 2 };
+
+// Work per lattice a launch maps CTAs onto.
+enum WorkKind { WORK_HALF = 0, WORK_SITES = 1, WORK_SPATIAL = 2, WORK_LINKS = 3 };
+
+template <int N> struct Ops {
+    // one checkerboard phase (parity, mu) of heatbath or overrelaxation;
+    // hb_offset is added to the lattice's pass counter (heatbath pass index
+    // inside the current sweep)
+    static cudaError_t update(int fp64, int layout, int mode, const BatchView& bv, int block,
+                              int parity, int mu, unsigned hb_offset, const InjView& inj, cudaStream_t s);
+    static cudaError_t cold(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
+    static cudaError_t hot(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
+    // FP64 reunitarization; only_due: skip lattices whose sweep counter is not
+    // a multiple of reunit_every
+    static cudaError_t reunit(int fp64, int layout, const BatchView& bv, int block, int only_due,
+                              cudaStream_t s);
+    // per-CTA partials: plaquette 2 values, polyakov 2, wilson 2(R+1)(T+1),
+    // unitarity 1 (max); partial layout [block][value][sum, compensation]
+    static cudaError_t plaquette(int fp64, int layout, const BatchView& bv, int block, double* partials,
+                                 cudaStream_t s);
+    static cudaError_t polyakov(int fp64, int layout, const BatchView& bv, int block, double* partials,
+                                cudaStream_t s);
+    static cudaError_t wilson(int fp64, int layout, const BatchView& bv, int block, int R, int T,
+                              double* partials, cudaStream_t s);
+    static cudaError_t unitarity(int fp64, int layout, const BatchView& bv, int block, double* partials,
+                                 cudaStream_t s);
+    // canonical FP64 host order (site-major, 4 dirs, N*N row-major) <-> image
+    static cudaError_t pack(int fp64, int layout, const BatchView& bv, int block, const void* canon,
+                            cudaStream_t s);
+    static cudaError_t unpack(int fp64, int layout, const BatchView& bv, int block, void* canon,
+                              cudaStream_t s);
+};
+
+extern template struct Ops<2>;
+extern template struct Ops<3>;
+extern template struct Ops<4>;
+extern template struct Ops<6>;
+
+// generic (N-independent) kernels, defined in engine.cu
+cudaError_t launch_finalize_sum(const BatchView& bv, const double* partials, int nvals, double* out,
+                                cudaStream_t s);
+cudaError_t launch_finalize_max(const BatchView& bv, const double* partials, double* out, cudaStream_t s);
+cudaError_t launch_end_sweep(const LatDev* lats, int nlat, unsigned n_hb, unsigned inc, cudaStream_t s);
+
+}  // namespace sunb
