@@ -1,10 +1,15 @@
 """GPU parity: the sm_100a engine (through the C ABI) against the FP64 oracle.
 
-Tolerances: FP64 lattices agree per link to 1e-11 (staples, updates and
-reunitarization differ from the oracle only by rounding); FP32 lattices to
-2e-5 per link after a full pass, with the oracle run on the same (FP32-stored)
-input; measurements, always computed in FP64, agree to 1e-12 on the same
-stored links and to 1e-6 between FP32 storage and the FP64 configuration.
+Tolerances (per link, max |difference| of complex entries): after one update
+pass FP64 lattices agree to 1e-11 (staples, updates and reunitarization differ
+from the oracle only by rounding) and FP32 lattices to 5e-5, with the oracle
+run in FP64 on the same FP32-stored input; the 8-parameter layout is looser
+(1e-10 / 5e-4) because its reconstruction divides by |e01|^2 + |e02|^2.
+Heatbath in FP32 may flip an accept/reject decision at the rounding boundary
+for under 1% of links.  Measurements, always computed in FP64, agree to 1e-12
+on the same stored links and to 1e-6 (8-parameter: 1e-5) between FP32 storage
+and the FP64 configuration.  Chains of sweeps are compared sweep by sweep:
+the dynamics amplifies rounding differences about a thousandfold per sweep.
 """
 import numpy as np
 import pytest
@@ -50,8 +55,20 @@ def _make(ctx, N, dims, prec, lay, beta=6.0, seed=1234, evenodd=True, reunit_eve
                  reunit_every=reunit_every)
 
 
-def _tol(prec):
-    return 1e-11 if prec == "f64" else 2e-5
+def _tol(prec, lay=0):
+    """Per-link tolerance after one update pass.  The 8-parameter form
+    rebuilds e00, e20 and the 2x2 minor through 1/(|e01|^2 + |e02|^2), which
+    amplifies the storage rounding where that norm is small."""
+    if prec == "f64":
+        return 1e-10 if lay == 2 else 1e-11
+    return 5e-4 if lay == 2 else 5e-5
+
+
+def _stol(prec, lay=0):
+    """Per-link tolerance of storage alone (store + reconstruct)."""
+    if prec == "f64":
+        return 1e-11 if lay == 2 else 1e-13
+    return 2e-4 if lay == 2 else 2e-6
 
 
 @pytest.mark.parametrize("case", ALL, ids=_ids)
@@ -61,7 +78,7 @@ def test_hot_start_matches_oracle(ctx, case):
     g.Init(hot=True)
     U = g.Get()
     ref = O.hot(N, list(dims), 77)
-    assert np.abs(U - ref).max() < (1e-13 if prec == "f64" else 2e-6)
+    assert np.abs(U - ref).max() < _stol(prec, lay)
 
 
 @pytest.mark.parametrize("case", [c for c in ALL if c[3] != 2], ids=_ids)
@@ -100,7 +117,7 @@ def test_measurements_match_oracle(ctx, case, evenodd):
     assert np.abs(w.real - wo[..., 0]).max() < 1e-12 and np.abs(w.imag - wo[..., 1]).max() < 1e-12
     # against the FP64 configuration itself: the storage error
     p64 = O.plaquette(U, X)
-    assert abs(p.real - p64[0]) < (1e-12 if prec == "f64" else 1e-6)
+    assert abs(p.real - p64[0]) < (1e-12 if prec == "f64" else (1e-5 if lay == 2 else 1e-6))
 
 
 @pytest.mark.parametrize("case", ALL, ids=_ids)
@@ -114,7 +131,7 @@ def test_overrelaxation_matches_oracle(ctx, case):
     OverRelaxation(g).Run(1)
     O.sweeps(ref, list(dims), beta, 0, 1, 1)
     got = g.Get()
-    assert np.abs(got - ref).max() < _tol(prec)
+    assert np.abs(got - ref).max() < _tol(prec, lay)
 
 
 def _mismatch(a, b, tol):
@@ -134,7 +151,7 @@ def test_heatbath_philox_matches_oracle(ctx, case):
     O.sweeps(ref, list(dims), beta, 1, 0, 1, mode=O.RNG_PHILOX64 if prec == "f64" else O.RNG_PHILOX32,
              seed=4242)
     got = g.Get()
-    frac, d = _mismatch(got, ref, _tol(prec))
+    frac, d = _mismatch(got, ref, _tol(prec, lay))
     # FP64: every link; FP32: an accept/reject decision at the rounding
     # boundary may flip for a handful of links
     assert frac == 0.0 if prec == "f64" else frac < 0.01, (frac, d.max())
@@ -161,7 +178,7 @@ def test_heatbath_injected_matches_oracle(ctx, case):
             assert O.update_phase(ref, list(dims), par, mu, 0, beta, O.RNG_INJECTED, inj=u,
                                   inj_stride=stride) == 0
     got = g.Get()
-    frac, d = _mismatch(got, ref, _tol(prec))
+    frac, d = _mismatch(got, ref, _tol(prec, lay))
     assert frac == 0.0 if prec == "f64" else frac < 0.01, (frac, d.max())
 
 
@@ -176,20 +193,28 @@ def test_heatbath_injected_overrun_flagged(ctx):
     assert e.value.status == 8
 
 
-@pytest.mark.parametrize("case", [c for c in ALL if c[3] == 0], ids=_ids)
+@pytest.mark.parametrize("case", [c for c in ALL if c[3] == 0 and c[2] == "f64"], ids=_ids)
 def test_sweeps_with_reunit_match_oracle(ctx, case):
+    """Full sweeps (1 HB + 4 OR, reunitarization every 2nd sweep) checked in
+    lockstep: the oracle restarts from the device state before every sweep.
+    The Monte Carlo dynamics amplifies rounding differences ~1e3-fold per
+    sweep, so a chain of sweeps can only be compared sweep by sweep, and only
+    in FP64: FP32 rounding (1e-7) grows past any per-link tolerance within
+    one 5-pass sweep for N >= 4 (FP32 is compared pass by pass above)."""
     from sun_b200 import Sweep
     N, dims, prec, lay = case
-    if prec == "f32":
-        pytest.skip("chained FP32 sweeps diverge from the FP64 chain by design")
     U, beta = _thermal(N, dims)
     g = _make(ctx, N, dims, prec, lay, beta=beta, seed=9, reunit_every=2)
     g.Set(U)
-    Sweep(g, 1, 4, 3)
-    p = O.sweeps(U, list(dims), beta, 1, 4, 3, reunit_every=2, seed=9)
-    assert p == 3
-    frac, d = _mismatch(g.Get(), U, 1e-10)
-    assert frac == 0.0, d.max()
+    mode = O.RNG_PHILOX64 if prec == "f64" else O.RNG_PHILOX32
+    for s in range(3):
+        ref = g.Get()
+        Sweep(g, 1, 4, 1)
+        reunit = 1 if (s + 1) % 2 == 0 else 0
+        p = O.sweeps(ref, list(dims), beta, 1, 4, 1, reunit_every=reunit, mode=mode, seed=9, pass_=s)
+        assert p == s + 1
+        frac, d = _mismatch(g.Get(), ref, 1e-8 if prec == "f64" else 2e-3)
+        assert frac == 0.0 if prec == "f64" else frac < 0.01, (s, frac, d.max())
     assert g.rng_state()[1:] == (3, 3)
 
 
@@ -206,6 +231,11 @@ def test_reunitarize_matches_oracle(ctx, case):
     Reunitarize(g).Run()
     O.reunitarize(stored, list(dims))
     got = g.Get()
+    if lay == 2:
+        # the 8-parameter form only encodes unitary matrices: a perturbed
+        # link is stored inconsistently, so only unitarity is checked
+        assert unitarity_violation(g) < _stol(prec, lay)
+        return
     assert np.abs(got - stored).max() < (1e-12 if prec == "f64" else 1e-6)
     assert unitarity_violation(g) < (1e-13 if prec == "f64" else 2e-6)
     assert abs(unitarity_violation(g) - O.unitarity_violation(got, list(dims))) < 1e-12
@@ -222,7 +252,7 @@ def test_layout_copy_roundtrip(ctx):
             for prec in ("f32", "f64"):
                 dst = gauge(ctx, N=3, dims=dims, atype=lay, evenodd=eo, prec=prec)
                 dst.Copy(src)
-                tol = 1e-12 if prec == "f64" else 2e-6
+                tol = _stol(prec, lay)
                 assert np.abs(dst.Get() - U).max() < tol
                 back = _make(ctx, 3, dims, "f64", 0)
                 back.Copy(dst)
