@@ -490,6 +490,16 @@ sun_status sun_init(const sun_config* cfg, sun_ctx** out)
         size_t fr = 0, tot = 0;
         ck(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
         c->hbm_budget = (cfg && cfg->hbm_budget_bytes) ? cfg->hbm_budget_bytes : (size_t)(0.9 * (double)fr);
+        // launch-shape overrides (CTA sizes, multiples of 32 up to 256)
+        auto env_blk = [](const char* name, int& v) {
+            if (const char* s = getenv(name)) {
+                int b = atoi(s);
+                if (b >= 32 && b <= 256 && b % 32 == 0) v = b;
+            }
+        };
+        env_blk("SUN_B200_BLOCK_UPDATE", c->blk_update);
+        env_blk("SUN_B200_BLOCK_SITES", c->blk_sites);
+        env_blk("SUN_B200_BLOCK_LINKS", c->blk_links);
         *out = c.release();
     });
 }

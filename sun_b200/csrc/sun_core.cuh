@@ -192,19 +192,32 @@ SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, St
 }
 
 // Microcanonical overrelaxation -- overrelaxationSUN
-// (include/device_PHB_OVR.h:494-608): conj-normalised block applied twice.
+// (include/device_PHB_OVR.h:494-608): per subgroup the conj-normalised block
+// element a is applied twice.  Here its square is applied once: for the
+// quaternion a = (a0, a1, a2, a3), a a = (a0^2 - |a_vec|^2, 2 a0 a_vec), the
+// same SU(2) element with half the row arithmetic.
+template <class R> SUN_DEV void su2_overrelax_element(const R r[4], R c[4])
+{
+    const R n2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3];
+    const R inv = R(1) / n2;
+    // a = (r0, -r1, -r2, -r3)/|r|  ->  a^2 = ((r0^2 - |r_vec|^2), -2 r0 r_vec) / |r|^2
+    const R t = R(-2) * r[0] * inv;
+    c[0] = (r[0] * r[0] - (r[1] * r[1] + r[2] * r[2] + r[3] * r[3])) * inv;
+    c[1] = t * r[1];
+    c[2] = t * r[2];
+    c[3] = t * r[3];
+}
+
 template <int N, class R> SUN_DEV void overrelax_update(Mat<N, R>& U, const Mat<N, R>& S)
 {
     if constexpr (N == 3) {
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
             const int p = SubGroup<3>::p(b), q = SubGroup<3>::q(b);
-            R r[4];
+            R r[4], c[4];
             su2_block_US<N, R>(U, S, p, q, r);
-            R n = R(1) / sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
-            r[0] *= n; r[1] *= -n; r[2] *= -n; r[3] *= -n;
-            su2_apply<N, R>(U, p, q, r);
-            su2_apply<N, R>(U, p, q, r);
+            su2_overrelax_element(r, c);
+            su2_apply<N, R>(U, p, q, c);
         }
     } else {
         Mat<N, R> M;
@@ -212,14 +225,11 @@ template <int N, class R> SUN_DEV void overrelax_update(Mat<N, R>& U, const Mat<
 #pragma unroll
         for (int b = 0; b < SubGroup<N>::count; ++b) {
             const int p = SubGroup<N>::p(b), q = SubGroup<N>::q(b);
-            R r[4];
+            R r[4], c[4];
             su2_block<N, R>(M, p, q, r);
-            R n = R(1) / sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
-            r[0] *= n; r[1] *= -n; r[2] *= -n; r[3] *= -n;
-            su2_apply<N, R>(U, p, q, r);
-            su2_apply<N, R>(U, p, q, r);
-            su2_apply<N, R>(M, p, q, r);
-            su2_apply<N, R>(M, p, q, r);
+            su2_overrelax_element(r, c);
+            su2_apply<N, R>(U, p, q, c);
+            su2_apply<N, R>(M, p, q, c);
         }
     }
 }
@@ -328,6 +338,13 @@ template <class R> SUN_DEV void rebuild8(Mat<3, R>& A, R th0, R th2)
 
 template <int N, class R, int LAYOUT> struct LinkIO {
     static constexpr int NE = LayoutInfo<N, LAYOUT>::elems;
+    // SOA12: the two stored rows only, row 2 left unset
+    template <bool NC> static SUN_DEV void load_rows(const cx<R>* base, uint32_t idx, uint32_t stride, Mat<N, R>& A)
+    {
+        static_assert(LAYOUT == L_SOA12, "stored rows exist for SOA12 only");
+#pragma unroll
+        for (int e = 0; e < 6; ++e) A.e[e / 3][e % 3] = ld_elem<R, NC>(base + idx + e * stride);
+    }
     template <bool NC> static SUN_DEV void load(const cx<R>* base, uint32_t idx, uint32_t stride, Mat<N, R>& A)
     {
         if constexpr (LAYOUT == L_SOA) {

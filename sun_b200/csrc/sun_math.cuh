@@ -127,6 +127,32 @@ template <int N, class R> SUN_HD void macc(const Mat<N, R>& A, const Mat<N, R>& 
             S.e[i][j] = s;
         }
 }
+// S += A^dagger B
+template <int N, class R> SUN_HD void macc_dn(const Mat<N, R>& A, const Mat<N, R>& B, Mat<N, R>& S)
+{
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            cx<R> s = S.e[i][j];
+#pragma unroll
+            for (int k = 0; k < N; ++k) s = cfma_cn(A.e[k][i], B.e[k][j], s);
+            S.e[i][j] = s;
+        }
+}
+// rows 0 and 1 of C = A B (only rows 0, 1 of A are read)
+template <class R> SUN_HD void mmul_rows01(const Mat<3, R>& A, const Mat<3, R>& B, Mat<3, R>& C)
+{
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            cx<R> s = A.e[i][0] * B.e[0][j];
+            s = cfma(A.e[i][1], B.e[1][j], s);
+            s = cfma(A.e[i][2], B.e[2][j], s);
+            C.e[i][j] = s;
+        }
+}
 template <int N, class R> SUN_HD cx<R> mtrace(const Mat<N, R>& A)
 {
     cx<R> t = A.e[0][0];

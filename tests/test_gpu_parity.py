@@ -2,7 +2,7 @@
 
 Tolerances (per link, max |difference| of complex entries): after one update
 pass FP64 lattices agree to 1e-11 (staples, updates and reunitarization differ
-from the oracle only by rounding) and FP32 lattices to 5e-5, with the oracle
+from the oracle only by rounding) and FP32 lattices to 1.2e-4, with the oracle
 run in FP64 on the same FP32-stored input; the 8-parameter layout is looser
 (1e-10 / 5e-4) because its reconstruction divides by |e01|^2 + |e02|^2.
 Heatbath in FP32 may flip an accept/reject decision at the rounding boundary
@@ -18,9 +18,10 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CASES = [  # (N, dims)
+CASES = [  # (N, dims); T % 4 == 0 takes the two-links-per-thread FP32 kernel
     (3, (4, 4, 4, 4)),
     (3, (4, 4, 4, 8)),
+    (3, (4, 4, 2, 6)),
     (2, (4, 4, 4, 4)),
     (4, (4, 4, 4, 4)),
     (6, (4, 4, 4, 4)),
@@ -61,7 +62,7 @@ def _tol(prec, lay=0):
     amplifies the storage rounding where that norm is small."""
     if prec == "f64":
         return 1e-10 if lay == 2 else 1e-11
-    return 5e-4 if lay == 2 else 5e-5
+    return 5e-4 if lay == 2 else 1.2e-4
 
 
 def _stol(prec, lay=0):
@@ -110,8 +111,9 @@ def test_measurements_match_oracle(ctx, case, evenodd):
     X = list(dims)
     p = PlaquetteCUB(g).Run()
     l = OnePolyakovLoop(g).Run()
-    w = WilsonLoop(g, 2, 3)
-    po, lo, wo = O.plaquette(stored, X), O.polyakov(stored, X), O.wilson_loops(stored, X, 2, 3)
+    R, T = min(2, min(dims[:3]) - 1), min(3, dims[3] - 1)
+    w = WilsonLoop(g, R, T)
+    po, lo, wo = O.plaquette(stored, X), O.polyakov(stored, X), O.wilson_loops(stored, X, R, T)
     assert abs(p.real - po[0]) < 1e-12 and abs(p.imag - po[1]) < 1e-12
     assert abs(l.real - lo[0]) < 1e-12 and abs(l.imag - lo[1]) < 1e-12
     assert np.abs(w.real - wo[..., 0]).max() < 1e-12 and np.abs(w.imag - wo[..., 1]).max() < 1e-12
@@ -213,7 +215,7 @@ def test_sweeps_with_reunit_match_oracle(ctx, case):
         reunit = 1 if (s + 1) % 2 == 0 else 0
         p = O.sweeps(ref, list(dims), beta, 1, 4, 1, reunit_every=reunit, mode=mode, seed=9, pass_=s)
         assert p == s + 1
-        frac, d = _mismatch(g.Get(), ref, 1e-8 if prec == "f64" else 2e-3)
+        frac, d = _mismatch(g.Get(), ref, 1e-7)
         assert frac == 0.0 if prec == "f64" else frac < 0.01, (s, frac, d.max())
     assert g.rng_state()[1:] == (3, 3)
 
@@ -370,3 +372,21 @@ def test_server_result_independent_of_mix(ctx):
     assert r1["plaquette"] == r2["plaquette"] and r1["polyakov"] == r2["polyakov"]
     assert r1["wilson"] == r2["wilson"]
     assert len(res2) == 4
+
+
+def test_batch_of_uneven_shapes_with_graph(ctx):
+    from sun_b200 import Batch, Sweep
+    batch, alone, mixed = Batch(ctx), [], []
+    for i, d in enumerate([(4, 4, 4, 8), (4, 4, 4, 6), (6, 6, 6, 12), (8, 8, 8, 10)]):
+        a = _make(ctx, 3, d, "f32", 1, seed=50 + i, beta=5.9)
+        b = _make(ctx, 3, d, "f32", 1, seed=50 + i, beta=5.9)
+        a.Init(hot=True)
+        b.Init(hot=True)
+        alone.append(a)
+        mixed.append(b)
+        batch.add(b)
+    for a in alone:
+        Sweep(a, 1, 4, 2)
+    batch.sweep(1, 4, 2, graph=True)
+    for a, b in zip(alone, mixed):
+        assert np.array_equal(a.get_image(), b.get_image())
