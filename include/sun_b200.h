@@ -126,6 +126,22 @@ sun_status sun_unitarity_violation(sun_lattice *lat, double *out, void *stream);
  * WilsonLoop<Real>(gauge, res, R, T) -> res[t + r(T+1)] complex
  *   (src/meas/wilsonloop.cu:535); R, T <= 8; any storage order accepted. */
 sun_status sun_plaquette(sun_lattice *lat, double out[2], void *stream);
+/* The plaquette for callers that cannot allocate device memory (no
+ * counterpart in the reference).  sun_plaquette() lets the library
+ * cudaMalloc its reduction scratch on first use; code capturing a CUDA graph,
+ * applications that own all device memory through their own pool, and hosts
+ * with a fixed memory budget cannot allow that.  This entry point allocates
+ * nothing: its scratch is a fixed 2 MiB array compiled into the library
+ * (held on every GPU that loads it), so lattices of at most 8,388,608 sites
+ * are accepted and larger ones are rejected with SUN_ERR_CAPACITY.
+ * d_links: device image with the layout, order and precision given in p
+ * (p->beta, p->seed, p->reunit_every are ignored); d_out: device memory for
+ * 2 doubles {spatial, temporal}, written asynchronously on `stream`.  The
+ * first call on each device looks up the scratch address (no allocation);
+ * make that first call before any stream capture.  All calls share the
+ * scratch: calls that overlap on the GPU race.  Errors: status code plus
+ * sun_last_error_string(NULL). */
+sun_status sun_plaquette_noalloc(const void *d_links, const sun_lattice_params *p, double *d_out, void *stream);
 sun_status sun_polyakov(sun_lattice *lat, double out[2], void *stream);
 sun_status sun_wilson_loops(sun_lattice *lat, int R, int T, double *out, void *stream);
 

@@ -72,6 +72,7 @@ _SIGS = {
     "sun_reunitarize": [_vp, _vp],
     "sun_unitarity_violation": [_vp, _dp, _vp],
     "sun_plaquette": [_vp, _dp, _vp],
+    "sun_plaquette_noalloc": [_vp, C.POINTER(SunLatticeParams), _vp, _vp],
     "sun_polyakov": [_vp, _dp, _vp],
     "sun_wilson_loops": [_vp, C.c_int, C.c_int, _dp, _vp],
     "sun_save_bin": [_vp, C.c_char_p, C.c_int, C.c_int],

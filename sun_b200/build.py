@@ -22,7 +22,7 @@ LIB = os.path.join(HERE, "libsun_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
               "-I" + os.path.join(ROOT, "include")] + ARCH
-UNITS = ["ops_n2.cu", "ops_n3.cu", "ops_n4.cu", "ops_n6.cu", "engine.cu", "server.cu"]
+UNITS = ["ops_n2.cu", "ops_n3.cu", "ops_n4.cu", "ops_n6.cu", "engine.cu", "server.cu", "noalloc.cu"]
 
 
 def _nvcc() -> str:

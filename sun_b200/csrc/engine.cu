@@ -336,6 +336,12 @@ sun_status handle(sun_ctx* c, const std::function<void()>& f);
 // Generic kernels (N-independent)
 namespace sunb {
 
+void set_global_error(const char* msg)
+{
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err = msg;
+}
+
 struct DDh { double s, c; };
 __device__ __forceinline__ DDh ddh_add(DDh a, DDh b)
 {

@@ -79,5 +79,7 @@ cudaError_t launch_finalize_sum(const BatchView& bv, const double* partials, int
                                 cudaStream_t s);
 cudaError_t launch_finalize_max(const BatchView& bv, const double* partials, double* out, cudaStream_t s);
 cudaError_t launch_end_sweep(const LatDev* lats, int nlat, unsigned n_hb, unsigned inc, cudaStream_t s);
+// message returned by sun_last_error_string(NULL)
+void set_global_error(const char* msg);
 
 }  // namespace sunb

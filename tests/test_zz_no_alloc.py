@@ -1,0 +1,71 @@
+"""The allocation-free plaquette entry point, sun_plaquette_noalloc.
+
+It exists for callers that cannot let a library call cudaMalloc: code that
+is capturing a CUDA graph, applications whose device memory all belongs to
+their own pool, and hosts with a fixed memory budget.  Its scratch is a fixed
+array compiled into the library; these tests call it through the C ABI and
+check it against the allocating sun_plaquette on two calls in a row.
+
+The file name sorts last so that a run stopping at the first failure has run
+every other test before this one.
+"""
+import ctypes as C
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(3, (8, 8, 8, 8), 1, "f32"), (3, (4, 4, 4, 8), 0, "f64"), (3, (4, 4, 4, 4), 2, "f64"),
+         (2, (4, 4, 4, 4), 0, "f32"), (4, (4, 4, 6, 4), 0, "f64"), (6, (4, 4, 4, 4), 0, "f32")]
+
+
+def _params(N, dims, lay, prec):
+    from sun_b200._native import SunLatticeParams
+    return SunLatticeParams(N, (C.c_int * 4)(*dims), 0.0, lay, 0, 1 if prec == "f64" else 0, 0, 0)
+
+
+@pytest.mark.parametrize("N,dims,lay,prec", CASES)
+def test_noalloc_plaquette_matches_allocating_entry_point(ctx, N, dims, lay, prec):
+    import torch
+    from sun_b200 import PlaquetteCUB, Sweep, gauge
+    from sun_b200._native import lib
+    g = gauge(ctx, N=N, dims=dims, beta={2: 2.3, 3: 5.9, 4: 10.5, 6: 25.0}[N], atype=lay, prec=prec, seed=3)
+    g.Init(hot=True)
+    p = _params(N, dims, lay, prec)
+    out = torch.full((2,), -1.0, dtype=torch.float64, device="cuda")
+    for call in range(2):
+        if call == 1:
+            Sweep(g, 1, 1, 1)  # a different configuration for the second call
+        torch.cuda.synchronize()
+        st = lib().sun_plaquette_noalloc(C.c_void_p(g.GetPtr()), C.byref(p), C.c_void_p(out.data_ptr()), None)
+        assert st == 0, lib().sun_last_error_string(None)
+        torch.cuda.synchronize()
+        got = out.cpu().tolist()
+        ref = PlaquetteCUB(g).Run()
+        assert abs(got[0] - ref.real) < 1e-12 and abs(got[1] - ref.imag) < 1e-12, (call, got, ref)
+
+
+def test_noalloc_plaquette_allocates_nothing(ctx):
+    import torch
+    from sun_b200 import gauge
+    from sun_b200._native import lib
+    g = gauge(ctx, N=3, dims=(8, 8, 8, 8), atype=1, prec="f32", seed=4)
+    g.Init(hot=True)
+    p = _params(3, (8, 8, 8, 8), 1, "f32")
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    args = (C.c_void_p(g.GetPtr()), C.byref(p), C.c_void_p(out.data_ptr()), None)
+    assert lib().sun_plaquette_noalloc(*args) == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert lib().sun_plaquette_noalloc(*args) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
+def test_noalloc_plaquette_rejects_oversized_lattice():
+    from sun_b200._native import lib
+    p = _params(3, (64, 64, 64, 64), 1, "f32")
+    dummy = C.c_void_p(16)  # never dereferenced: the size check comes first
+    assert lib().sun_plaquette_noalloc(dummy, C.byref(p), dummy, None) == 7  # SUN_ERR_CAPACITY
+    assert b"exceed the fixed scratch" in lib().sun_last_error_string(None)
