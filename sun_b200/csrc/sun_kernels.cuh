@@ -49,6 +49,32 @@ SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
 }
 
 // ---------------------------------------------------------------------------
+// Register caps of the update kernel (CTAs of 128 threads that must fit on an
+// SM).  The update is latency-bound at the register-limited occupancy; for
+// SU(3) overrelaxation a cap of 80 registers (6 CTAs, 24 warps per SM) was
+// measured fastest on B200.
+#ifndef SUN_OCC_F32_OR
+#define SUN_OCC_F32_OR 6
+#endif
+#ifndef SUN_OCC_F32_HB
+#define SUN_OCC_F32_HB 1
+#endif
+#ifndef SUN_OCC_F64_OR
+#define SUN_OCC_F64_OR 1
+#endif
+#ifndef SUN_OCC_F64_HB
+#define SUN_OCC_F64_HB 1
+#endif
+template <int N, class R, int MODE> struct UpdateOccupancy {
+    static constexpr int min_blocks = 1;
+};
+template <class R, int MODE> struct UpdateOccupancy<3, R, MODE> {
+    static constexpr bool f32 = sizeof(R) == 4;
+    static constexpr int min_blocks = MODE == MODE_OR ? (f32 ? SUN_OCC_F32_OR : SUN_OCC_F64_OR)
+                                                      : (f32 ? SUN_OCC_F32_HB : SUN_OCC_F64_HB);
+};
+
+// ---------------------------------------------------------------------------
 // Checkerboard update of the links (x, mu) with parity(x) == parity --
 // kernel_PHeatBath_evenodd (src/monte/monte.cu:44-88) and
 // kernel_overrelaxation_evenodd (src/monte/ovr.cu:41-80).  One thread per
@@ -56,10 +82,7 @@ SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
 // "up" then "down"); neighbour links are read through the read-only path
 // (they are never written in this phase), the own link through plain loads.
 template <int N, class R, int LAYOUT, int MODE>
-#ifndef SUN_UPDATE_MIN_BLOCKS
-#define SUN_UPDATE_MIN_BLOCKS 1
-#endif
-__global__ void __launch_bounds__(128, SUN_UPDATE_MIN_BLOCKS) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
+__global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
                                                 InjView inj)
 {
     const int b = blockIdx.x;
