@@ -92,12 +92,22 @@ template <class R> struct InjectedStream {
 // a random direction.  Draw order: xr1, xr2, xr3, xr4 per KP try, xr1, xr2
 // per Creutz try, then one uniform for a3 and one for the azimuth.
 template <class R> struct MathFns;
+// FP32 draws use the hardware approximations (absolute error ~1e-6 on these
+// arguments, below the FP32 storage rounding of the links they feed); the
+// angle 2 pi u is shifted into [-pi, pi], where __sincosf is accurate:
+// cos(2 pi u) = -cos(2 pi (u - 1/2)), sin(2 pi u) = -sin(2 pi (u - 1/2)).
 template <> struct MathFns<float> {
-    static SUN_DEV float log_(float x) { return logf(x); }
-    static SUN_DEV float exp_(float x) { return expf(x); }
+    static SUN_DEV float log_(float x) { return __logf(x); }
+    static SUN_DEV float exp_(float x) { return __expf(x); }
     static SUN_DEV float sqrt_(float x) { return sqrtf(x); }
-    static SUN_DEV void sincos2pi(float u, float* s, float* c) { sincospif(2.0f * u, s, c); }
-    static SUN_DEV float cos2pi(float u) { return cospif(2.0f * u); }
+    static SUN_DEV void sincos2pi(float u, float* s, float* c)
+    {
+        float ss, cc;
+        __sincosf(6.28318530717958648f * (u - 0.5f), &ss, &cc);
+        *s = -ss;
+        *c = -cc;
+    }
+    static SUN_DEV float cos2pi(float u) { return -__cosf(6.28318530717958648f * (u - 0.5f)); }
 };
 template <> struct MathFns<double> {
     static SUN_DEV double log_(double x) { return log(x); }
@@ -158,18 +168,24 @@ template <int N, class R, class Stream>
 SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, Stream& st)
 {
     if constexpr (N == 3) {
-#pragma unroll
+        // one copy of the (large) SU(2) draw in a rolled loop over the three
+        // subgroups; the block extraction and row update switch on the
+        // subgroup so the matrices keep static (register) indexing
+#pragma unroll 1
         for (int b = 0; b < 3; ++b) {
-            const int p = SubGroup<3>::p(b), q = SubGroup<3>::q(b);
             R r[4], a[4], c[4];
-            su2_block_US<N, R>(U, S, p, q, r);
+            if (b == 0) su2_block_US<N, R>(U, S, 0, 1, r);
+            else if (b == 1) su2_block_US<N, R>(U, S, 1, 2, r);
+            else su2_block_US<N, R>(U, S, 0, 2, r);
             R k = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
             R ap = beta_over_n * k;
             k = R(1) / k;
             r[0] *= k; r[1] *= k; r[2] *= k; r[3] *= k;
             su2_heatbath_draw<R>(ap, st, a);
             su2_mul_udag(a, r, c);
-            su2_apply<N, R>(U, p, q, c);
+            if (b == 0) su2_apply<N, R>(U, 0, 1, c);
+            else if (b == 1) su2_apply<N, R>(U, 1, 2, c);
+            else su2_apply<N, R>(U, 0, 2, c);
         }
     } else {
         Mat<N, R> M;
