@@ -95,6 +95,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks_dist(x, world, device):
+    """Max of a per-rank number over all ranks (the job time of weak-scaled
+    replicas is the slowest rank's); identity for one rank."""
+    if world == 1:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seed(rank):
+    """Each rank advances its own independent lattice (replicas: the sweep
+    of one lattice does not shard without a halo exchange)."""
+    return SEED + rank
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -183,14 +200,10 @@ def main():
             torch.distributed.barrier()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_dist(x, world, "cuda")
 
     V = DIMS[0] * DIMS[1] * DIMS[2] * DIMS[3]
-    g = gauge(ctx, N=N, dims=DIMS, beta=BETA, atype=1, evenodd=True, prec="f32", seed=SEED + rank,
+    g = gauge(ctx, N=N, dims=DIMS, beta=BETA, atype=1, evenodd=True, prec="f32", seed=replica_seed(rank),
               reunit_every=REUNIT)
     g.Init(hot=True)
 
@@ -274,6 +287,8 @@ def main():
                                     "hbm_gbs_model": 20 * V * k64 * 9 * 144 / t64 / 1e9}
         g64.Release()
         extras["batched"] = batched_bench(ctx, L, sp, stream, args)
+        if rank == 0:
+            extras["serving"] = serving_bench(ctx)
 
     line = {
         "metric": "link-updates/s",
@@ -323,6 +338,61 @@ def main():
     ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def serving_jobs(rate=50.0, window=4.0, seed=1234):
+    """Poisson arrivals (mean `rate` per second over `window` seconds) of jobs
+    with N in {2,3,4}, L^3 x T with L in {8..24} even and T in {L, 2L}, beta
+    uniform in a confined-phase range per N, 50..500 sweeps of 1 HB + 4 OR and
+    a random non-empty subset of {plaquette, Polyakov loop, Wilson loops up
+    to 4x4}; FP32 links (12-parameter for SU(3))."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    beta_range = {2: (2.0, 2.3), 3: (5.7, 5.9), 4: (10.2, 10.6)}
+    t, jobs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > window:
+            return jobs
+        n = int(rng.choice([2, 3, 4]))
+        l = int(rng.choice(np.arange(8, 25, 2)))
+        tt = int(rng.choice([l, 2 * l]))
+        obs = int(rng.integers(1, 8))
+        jobs.append(dict(t=t, N=n, dims=(l, l, l, tt), beta=float(rng.uniform(*beta_range[n])),
+                         sweeps=int(rng.integers(50, 501)), seed=int(rng.integers(1, 2 ** 62)), observables=obs,
+                         R=4 if obs & 4 else 0, T=4 if obs & 4 else 0))
+
+
+def serving_bench(ctx, rate=50.0, window=3.0, max_active=256):
+    """Continuous-batching server under the Poisson stream: jobs are submitted
+    at their arrival times while earlier ones run; p50/p99 latency (submit to
+    result) and aggregate link-updates/s over the run."""
+    import numpy as np
+    from sun_b200 import SOA, SOA12, Server, make_job
+    jobs = serving_jobs(rate, window)
+    srv = Server(ctx, max_active=max_active)
+    t0 = time.perf_counter()
+    pending, results, nxt = list(jobs), [], 0
+    while len(results) < len(jobs):
+        now = time.perf_counter() - t0
+        while nxt < len(pending) and pending[nxt]["t"] <= now:
+            j = pending[nxt]
+            srv.submit(make_job(N=j["N"], dims=j["dims"], beta=j["beta"], sweeps=j["sweeps"], seed=j["seed"],
+                                observables=j["observables"], R=j["R"], T=j["T"], prec="f32",
+                                layout=SOA12 if j["N"] == 3 else SOA, reunit_every=10))
+            nxt += 1
+        done = srv.step()
+        results += done
+        if not done and srv.pending() == (0, 0) and nxt < len(pending):
+            time.sleep(max(0.0, min(0.01, pending[nxt]["t"] - (time.perf_counter() - t0))))
+    wall = time.perf_counter() - t0
+    srv.close()
+    ok = [r for r in results if r["status"] == 0]
+    lat = np.array([r["finish_s"] - r["submit_s"] for r in ok])
+    upd = sum(r["link_updates"] for r in ok)
+    return {"jobs": len(jobs), "completed": len(ok), "arrival_rate_per_s": rate, "window_s": window,
+            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+            "link_updates_per_s": upd / wall, "wall_s": wall, "max_active": max_active}
 
 
 def batched_bench(ctx, L, sp, stream, args):

@@ -154,7 +154,12 @@ struct Group {
     int N = 0, fp64 = 0, layout = 0;
     std::vector<sun_lattice*> lats;
     DevBuf d_lats;
-    std::map<std::pair<int, int>, std::pair<std::shared_ptr<DevBuf>, int>> begins;
+    struct Begin {
+        std::shared_ptr<DevBuf> buf;  // CTA prefix, grows only
+        int nblocks = 0;
+        bool valid = false;
+    };
+    std::map<std::pair<int, int>, Begin> begins;
     DevBuf partials, out;
     PinnedBuf h_out;
     bool dirty = true;
@@ -178,29 +183,29 @@ struct Group {
             ck(cudaMemcpyAsync(d_lats.p, h.data(), sizeof(LatDev) * h.size(), cudaMemcpyHostToDevice, s),
                "table upload");
         ck(cudaStreamSynchronize(s), "table upload");
-        begins.clear();
+        for (auto& kv : begins) kv.second.valid = false;
         dirty = false;
     }
     BatchView view(int kind, int block, cudaStream_t s)
     {
         sync(s);
-        auto key = std::make_pair(kind, block);
-        auto it = begins.find(key);
-        if (it == begins.end()) {
+        Begin& e = begins[std::make_pair(kind, block)];
+        if (!e.valid) {
             std::vector<int> b(lats.size() + 1, 0);
             for (size_t i = 0; i < lats.size(); ++i)
                 b[i + 1] = b[i] + (work_of(lats[i]->desc, kind) + block - 1) / block;
-            auto buf = std::make_shared<DevBuf>();
-            buf->ensure(sizeof(int) * b.size());
-            ck(cudaMemcpyAsync(buf->p, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, s), "begin upload");
+            if (!e.buf) e.buf = std::make_shared<DevBuf>();
+            e.buf->ensure(sizeof(int) * b.size());
+            ck(cudaMemcpyAsync(e.buf->p, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, s), "begin upload");
             ck(cudaStreamSynchronize(s), "begin upload");
-            it = begins.emplace(key, std::make_pair(buf, b.back())).first;
+            e.nblocks = b.back();
+            e.valid = true;
         }
         BatchView v;
         v.lats = reinterpret_cast<const LatDev*>(d_lats.p);
-        v.begin = reinterpret_cast<const int*>(it->second.first->p);
+        v.begin = reinterpret_cast<const int*>(e.buf->p);
         v.nlat = (int)lats.size();
-        v.nblocks = it->second.second;
+        v.nblocks = e.nblocks;
         return v;
     }
 };
@@ -902,10 +907,16 @@ struct sun_batch {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
     }
+    // Regroup after membership changes.  Groups (and their device tables and
+    // scratch, which only grow) are kept per class and refilled, so a server
+    // that adds and retires lattices every step does not reallocate them.
     void regroup()
     {
         if (!dirty) return;
-        groups.clear();
+        for (auto& g : groups) {
+            g->lats.clear();
+            g->dirty = true;
+        }
         for (auto* l : order) {
             int fp64 = l->p.precision == SUN_F64, lay = l->p.layout;
             Group* g = nullptr;
@@ -1033,6 +1044,7 @@ static sun_status batch_measure(sun_batch* b, double* out, void* stream, bool pl
         b->regroup();
         cudaStream_t s = S(b->ctx, stream);
         for (auto& g : b->groups) {
+            if (g->lats.empty()) continue;
             std::vector<double> r(2 * g->lats.size());
             if (plaq) group_plaquette(b->ctx, *g, r.data(), s);
             else group_polyakov(b->ctx, *g, r.data(), s);
