@@ -81,6 +81,10 @@ sun_status sun_init(const sun_config *cfg, sun_ctx **out);
 sun_status sun_finalize(sun_ctx *ctx);
 const char *sun_last_error_string(const sun_ctx *ctx);
 const char *sun_version(void);
+/* host-side fault injection for tests (no reference counterpart): after
+ * after_n more device allocations succeed, every further one reports
+ * SUN_ERR_OUT_OF_MEMORY without calling the allocator; -1 turns it off */
+sun_status sun_debug_fail_allocations(int after_n);
 
 /* ---- gauge arrays: _gauge<Real>(ArrayType, Device, 4V, evenodd) + Allocate
  * (include/gaugearray.h:139, :603) with SETPARAMS geometry
@@ -119,6 +123,10 @@ sun_status sun_heatbath_injected(sun_lattice *lat, const double *dev_uniforms, i
 sun_status sun_reunitarize(sun_lattice *lat, void *stream);
 /* max over links of max_ij |(U^dag U - 1)_ij| */
 sun_status sun_unitarity_violation(sun_lattice *lat, double *out, void *stream);
+/* link diagnostics: GaugeTraceCUB (src/meas/linktrsum.cu:146, mean tr U / N)
+ * and GaugeDetCUB (src/meas/linkdetsum.cu:115, mean det U) in one pass:
+ * out = {Re, Im of mean tr U / N, Re, Im of mean det U} */
+sun_status sun_link_trace_det(sun_lattice *lat, double out[4], void *stream);
 
 /* ---- measurements (FP64 results, deterministic compensated sums) ----
  * PlaquetteCUB<Real>::Run -> {spatial, temporal} (src/meas/plaquette_cub.cu:226)

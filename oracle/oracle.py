@@ -69,6 +69,7 @@ def _declare(L: C.CDLL) -> None:
     L.orc_reunitarize.argtypes = [C.c_int, _ip, _dp]
     L.orc_unitarity_violation.argtypes = [C.c_int, _ip, _dp]
     L.orc_unitarity_violation.restype = C.c_double
+    L.orc_link_trace_det.argtypes = [C.c_int, _ip, _dp, _dp]
     L.orc_plaquette.argtypes = [C.c_int, _ip, _dp, _dp]
     L.orc_polyakov.argtypes = [C.c_int, _ip, _dp, _dp]
     L.orc_wilson_loops.argtypes = [C.c_int, _ip, _dp, C.c_int, C.c_int, _dp]
@@ -194,6 +195,12 @@ def reunitarize(U, X):
 
 def unitarity_violation(U, X) -> float:
     return lib().orc_unitarity_violation(U.shape[-1], _dims(X), _d(U))
+
+
+def link_trace_det(U, X):
+    o = np.zeros(4)
+    lib().orc_link_trace_det(U.shape[-1], _dims(X), _d(U), _d(o))
+    return o
 
 
 def plaquette(U, X):

@@ -546,6 +546,25 @@ void orc_sweeps(int N, const int X[4], double *U, double beta, int n_hb, int n_o
     }
 }
 
+/* Mean link trace / N and mean link determinant -- the sums of GaugeTraceCUB
+ * (src/meas/linktrsum.cu:56, normalised :146 by 4 N V) and GaugeDetCUB
+ * (src/meas/linkdetsum.cu:62, normalised :115 by 4 V).
+ * out = {Re tr/N, Im tr/N, Re det, Im det}. */
+void orc_link_trace_det(int N, const int X[4], const double *Ud, double out[4])
+{
+    const cplx *U = (const cplx *)Ud;
+    int V = X[0] * X[1] * X[2] * X[3];
+    cplx tr = 0, det = 0;
+    for (int l = 0; l < 4 * V; ++l) {
+        tr += mat_trace(N, U + (size_t)l * N * N);
+        det += mat_det(N, U + (size_t)l * N * N);
+    }
+    out[0] = creal(tr) / (4.0 * N * V);
+    out[1] = cimag(tr) / (4.0 * N * V);
+    out[2] = creal(det) / (4.0 * V);
+    out[3] = cimag(det) / (4.0 * V);
+}
+
 double orc_unitarity_violation(int N, const int X[4], const double *Ud)
 {
     const cplx *U = (const cplx *)Ud;

@@ -77,6 +77,7 @@ void orc_sweeps(int N, const int X[4], double *U, double beta, int n_hb, int n_o
                 int nthreads);
 void orc_reunitarize(int N, const int X[4], double *U);
 double orc_unitarity_violation(int N, const int X[4], const double *U);
+void orc_link_trace_det(int N, const int X[4], const double *U, double out[4]);
 
 /* --- measurements -----------------------------------------------------------*/
 void orc_plaquette(int N, const int X[4], const double *U, double out[2]);

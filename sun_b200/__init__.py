@@ -6,6 +6,7 @@ C ABI of ``include/sun_b200.h``); this package is its Python host binding.
 from ._native import SunError, lib  # noqa: F401
 from .api import (SOA, SOA8, SOA12, Batch, Context, EndCULQCD, HeatBath, OnePolyakovLoop,  # noqa: F401
                   OverRelaxation, PlaquetteCUB, ReadBin_Gauge, Reunitarize, SaveBin_Gauge, Server, Sweep,
-                  WilsonLoop, admit_count, gauge, initCULQCD, job_footprint, make_job, unitarity_violation)
+                  WilsonLoop, admit_count, gauge, initCULQCD, job_footprint, link_trace_det, make_job,
+                  unitarity_violation)
 
 __version__ = "0.1.0"

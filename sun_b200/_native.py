@@ -71,6 +71,8 @@ _SIGS = {
     "sun_heatbath_injected": [_vp, _vp, C.c_int, _vp],
     "sun_reunitarize": [_vp, _vp],
     "sun_unitarity_violation": [_vp, _dp, _vp],
+    "sun_link_trace_det": [_vp, _dp, _vp],
+    "sun_debug_fail_allocations": [C.c_int],
     "sun_plaquette": [_vp, _dp, _vp],
     "sun_plaquette_noalloc": [_vp, C.POINTER(SunLatticeParams), _vp, _vp],
     "sun_polyakov": [_vp, _dp, _vp],

@@ -50,8 +50,9 @@ class Context:
     """initCULQCD / EndCULQCD: one device, one default stream."""
 
     def __init__(self, device: int = 0, verbosity: int = 0, tune: bool = False,
-                 hbm_budget_bytes: int = 0):
-        cfg = nat.SunConfig(device, verbosity, int(tune), None, hbm_budget_bytes)
+                 hbm_budget_bytes: int = 0, tune_cache_path: Optional[str] = None):
+        self._tune_path = tune_cache_path.encode() if tune_cache_path else None
+        cfg = nat.SunConfig(device, verbosity, int(tune), self._tune_path, hbm_budget_bytes)
         h = C.c_void_p()
         check(lib().sun_init(C.byref(cfg), C.byref(h)))
         self.h = h
@@ -200,6 +201,14 @@ def unitarity_violation(g: gauge) -> float:
     v = C.c_double()
     check(lib().sun_unitarity_violation(g.h, C.byref(v), None), g.ctx.h)
     return v.value
+
+
+def link_trace_det(g: gauge):
+    """(mean tr U / N, mean det U) as complex numbers -- GaugeTraceCUB and
+    GaugeDetCUB (src/meas/linktrsum.cu, src/meas/linkdetsum.cu)."""
+    o = (C.c_double * 4)()
+    check(lib().sun_link_trace_det(g.h, o, None), g.ctx.h)
+    return complex(o[0], o[1]), complex(o[2], o[3])
 
 
 class PlaquetteCUB:

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -53,6 +54,10 @@ void ck(cudaError_t e, const char* what)
     if (e != cudaSuccess) fail(SUN_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
+// Host-side fault injection (sun_debug_fail_allocations): allocations left
+// before every further device allocation reports out-of-memory; -1 = off.
+std::atomic<int> g_alloc_budget{-1};
+
 // Device buffer owned by the library.
 struct DevBuf {
     void* p = nullptr;
@@ -71,6 +76,10 @@ struct DevBuf {
     {
         if (bytes <= n) return;
         release();
+        int left = g_alloc_budget.load();
+        while (left > 0 && !g_alloc_budget.compare_exchange_weak(left, left - 1)) {
+        }
+        if (left == 0) fail(SUN_ERR_OUT_OF_MEMORY, "cudaMalloc: out of memory (injected)");
         ck(cudaMalloc(&p, bytes), "cudaMalloc");
         n = bytes;
     }
@@ -119,6 +128,11 @@ struct sun_ctx {
     size_t hbm_budget = 0;
     // launch shapes (CTA sizes) per kernel family
     int blk_update = 128, blk_sites = 128, blk_links = 256, blk_wilson = 64;
+    // autotuner (tuneLaunch, src/tune.cpp:304): CTA size of the update kernel
+    // per (kernel class, total half-volume), timed once, cached in a CSV file
+    bool tune = false;
+    std::string tune_path;
+    std::map<std::string, int> tuned;
 };
 
 namespace { struct Group; }
@@ -224,19 +238,88 @@ struct Group {
     } while (0)
 
 // -- sweeps ------------------------------------------------------------------
+// CTA size of the update kernel for this group and mode.  With tuning on,
+// the first use of a (class, mode, total half-volume) key times one phase
+// launch per candidate size on the real lattices -- links backed up before and
+// restored after, like Tunable::preTune/postTune (include/tune.h:119,
+// monte.h:73-74) -- keeps the fastest and appends it to the cache file.
+int update_block(sun_ctx* c, Group& g, int mode, cudaStream_t s)
+{
+    if (!c->tune) return c->blk_update;
+    long long work = 0;
+    size_t bytes = 0;
+    for (auto* l : g.lats) {
+        work += l->desc.halfV;
+        bytes += l->bytes;
+    }
+    char key[160];
+    snprintf(key, sizeof key, "k_update N=%d %s layout=%d mode=%d halfV=%lld", g.N, g.fp64 ? "f64" : "f32", g.layout,
+             mode, work);
+    auto it = c->tuned.find(key);
+    if (it != c->tuned.end()) return it->second;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return c->blk_update;
+    DevBuf backup;
+    backup.ensure(bytes);
+    size_t off = 0;
+    for (auto* l : g.lats) {
+        ck(cudaMemcpyAsync((char*)backup.p + off, l->links.p, l->bytes, cudaMemcpyDeviceToDevice, s), "tune backup");
+        off += l->bytes;
+    }
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    InjView none{nullptr, 0, nullptr};
+    int best = c->blk_update;
+    float best_ms = 1e30f;
+    for (int blk : {32, 64, 96, 128}) {
+        BatchView v = g.view(WORK_HALF, blk, s);
+        OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, blk, 0, 0, 0u, none, s);  // warm-up
+        ck(cudaEventRecord(e0, s), "event");
+        for (int r = 0; r < 3; ++r) OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, blk, 0, 0, 0u, none, s);
+        ck(cudaEventRecord(e1, s), "event");
+        ck(cudaEventSynchronize(e1), "event");
+        float ms = 0;
+        ck(cudaEventElapsedTime(&ms, e0, e1), "event");
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = blk;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    off = 0;
+    for (auto* l : g.lats) {
+        ck(cudaMemcpyAsync(l->links.p, (char*)backup.p + off, l->bytes, cudaMemcpyDeviceToDevice, s), "tune restore");
+        off += l->bytes;
+    }
+    ck(cudaStreamSynchronize(s), "tune restore");
+    c->tuned[key] = best;
+    if (!c->tune_path.empty()) {
+        if (FILE* f = fopen(c->tune_path.c_str(), "a")) {
+            fprintf(f, "%s,%d,%.6f\n", key, best, best_ms / 3.0);
+            fclose(f);
+        }
+    }
+    return best;
+}
+
 void group_sweep(sun_ctx* c, Group& g, int n_hb, int n_or, bool count_sweep, bool reunit, cudaStream_t s)
 {
     if (g.lats.empty()) return;
-    BatchView half = g.view(WORK_HALF, c->blk_update, s);
     InjView none{nullptr, 0, nullptr};
+    const int bhb = n_hb > 0 ? update_block(c, g, MODE_HB, s) : c->blk_update;
+    const int bor = n_or > 0 ? update_block(c, g, MODE_OR, s) : c->blk_update;
+    BatchView vhb = g.view(WORK_HALF, bhb, s);
     for (int h = 0; h < n_hb; ++h)
         for (int par = 0; par < 2; ++par)
             for (int mu = 0; mu < 4; ++mu)
-                OPS_CALL(g.N, update, g.fp64, g.layout, MODE_HB, half, c->blk_update, par, mu, (unsigned)h, none, s);
+                OPS_CALL(g.N, update, g.fp64, g.layout, MODE_HB, vhb, bhb, par, mu, (unsigned)h, none, s);
+    BatchView vor = g.view(WORK_HALF, bor, s);
     for (int o = 0; o < n_or; ++o)
         for (int par = 0; par < 2; ++par)
             for (int mu = 0; mu < 4; ++mu)
-                OPS_CALL(g.N, update, g.fp64, g.layout, MODE_OR, half, c->blk_update, par, mu, 0u, none, s);
+                OPS_CALL(g.N, update, g.fp64, g.layout, MODE_OR, vor, bor, par, mu, 0u, none, s);
     if (n_hb > 0 || count_sweep)
         ck(launch_end_sweep(reinterpret_cast<const LatDev*>(g.d_lats.p), (int)g.lats.size(), (unsigned)n_hb,
                             count_sweep ? 1u : 0u, s),
@@ -478,6 +561,12 @@ extern "C" {
 
 const char* sun_version(void) { return "sun_b200 0.1 (sm_100a)"; }
 
+sun_status sun_debug_fail_allocations(int after_n)
+{
+    g_alloc_budget.store(after_n < 0 ? -1 : after_n);
+    return SUN_OK;
+}
+
 const char* sun_last_error_string(const sun_ctx* c)
 {
     if (c) return c->last_error.c_str();
@@ -490,6 +579,21 @@ sun_status sun_init(const sun_config* cfg, sun_ctx** out)
         if (!out) fail(SUN_ERR_INVALID_ARG, "null output");
         auto c = std::make_unique<sun_ctx>();
         c->device = cfg ? cfg->device : 0;
+        c->tune = cfg && cfg->tune;
+        if (cfg && cfg->tune_cache_path) {
+            c->tune_path = cfg->tune_cache_path;
+            if (FILE* f = fopen(cfg->tune_cache_path, "r")) {  // "key,block,ms" lines
+                char line[256];
+                while (fgets(line, sizeof line, f)) {
+                    char* c1 = strchr(line, ',');
+                    if (!c1) continue;
+                    *c1 = 0;
+                    int blk = atoi(c1 + 1);
+                    if (blk >= 32 && blk <= 128 && blk % 32 == 0) c->tuned[line] = blk;
+                }
+                fclose(f);
+            }
+        }
         c->verbosity = cfg ? cfg->verbosity : 0;
         int n = 0;
         ck(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
@@ -787,6 +891,23 @@ sun_status sun_unitarity_violation(sun_lattice* l, double* out, void* stream)
     });
 }
 
+sun_status sun_link_trace_det(sun_lattice* l, double out[4], void* stream)
+{
+    if (!l || !out) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        cudaStream_t s = S(l->ctx, stream);
+        Solo so(l);
+        double* r = group_reduce(so.g, WORK_LINKS, 256, 4, false, s, [&](const BatchView& v, double* part) {
+            OPS_CALL(l->p.ncolors, linkstats, so.g.fp64, so.g.layout, v, 256, part, s);
+        });
+        const double nl = 4.0 * (double)l->desc.V;
+        out[0] = r[0] / (nl * l->p.ncolors);
+        out[1] = r[1] / (nl * l->p.ncolors);
+        out[2] = r[2] / nl;
+        out[3] = r[3] / nl;
+    });
+}
+
 sun_status sun_plaquette(sun_lattice* l, double out[2], void* stream)
 {
     if (!l || !out) return SUN_ERR_INVALID_ARG;
@@ -1010,7 +1131,10 @@ sun_status sun_batch_sweep(sun_batch* b, int n_hb, int n_or, int n_sweeps, int u
             b->drop_graph();
             // tables must exist before capture (their uploads synchronise)
             for (auto& g : b->groups) {
-                g->view(WORK_HALF, b->ctx->blk_update, s);
+                if (g->lats.empty()) continue;
+                // launch shapes (tuned if tuning is on) and their tables, before capture
+                if (n_hb > 0) g->view(WORK_HALF, update_block(b->ctx, *g, MODE_HB, s), s);
+                if (n_or > 0) g->view(WORK_HALF, update_block(b->ctx, *g, MODE_OR, s), s);
                 g->view(WORK_LINKS, b->ctx->blk_links, s);
             }
             cudaStream_t cs;

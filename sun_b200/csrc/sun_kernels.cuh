@@ -531,6 +531,35 @@ __global__ void __launch_bounds__(64) k_wilson(BatchView bv, int RR, int TT, dou
 
 // max over links of max_ij |(U^dag U - 1)_ij| (FP64)
 template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(256) k_unitarity(BatchView bv, double* partials);
+
+// Link diagnostics -- the sums of GaugeTraceCUB / GaugeDetCUB
+// (src/meas/linktrsum.cu, src/meas/linkdetsum.cu): per link tr U and det U in
+// FP64, four compensated sums (Re tr, Im tr, Re det, Im det) per CTA.
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(256) k_linkstats(BatchView bv, double* partials)
+{
+    __shared__ DD sh[32];
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (w < 4 * L.V) {
+        Mat<N, R> A;
+        LinkIO<N, R, LAYOUT>::template load<true>(reinterpret_cast<const cx<R>*>(L.links), (uint32_t)w, 4u * L.V,
+                                                  A);
+        Mat<N, double> D;
+        mconvert(A, D);
+        const cx<double> t = mtrace(D);
+        const cx<double> d = mdet<N, double>(D);
+        v[0] = t.re; v[1] = t.im; v[2] = d.re; v[3] = d.im;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) block_sum(v[k], partials + ((size_t)b * 4 + k) * 2, sh);
+}
+
+template <int N, class R, int LAYOUT>
 __global__ void __launch_bounds__(256) k_unitarity(BatchView bv, double* partials)
 {
     __shared__ double sh[32];
@@ -700,6 +729,16 @@ cudaError_t Ops<N>::unitarity(int fp64, int layout, const BatchView& bv, int blo
                               cudaStream_t s)
 {
 #define CALL(R_, L_) k_unitarity<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::linkstats(int fp64, int layout, const BatchView& bv, int block, double* partials,
+                              cudaStream_t s)
+{
+#define CALL(R_, L_) k_linkstats<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
     return cudaGetLastError();

@@ -62,6 +62,9 @@ template <int N> struct Ops {
                               double* partials, cudaStream_t s);
     static cudaError_t unitarity(int fp64, int layout, const BatchView& bv, int block, double* partials,
                                  cudaStream_t s);
+    // sums of tr U and det U over links: 4 values (Re tr, Im tr, Re det, Im det)
+    static cudaError_t linkstats(int fp64, int layout, const BatchView& bv, int block, double* partials,
+                                 cudaStream_t s);
     // canonical FP64 host order (site-major, 4 dirs, N*N row-major) <-> image
     static cudaError_t pack(int fp64, int layout, const BatchView& bv, int block, const void* canon,
                             cudaStream_t s);

@@ -390,3 +390,51 @@ def test_batch_of_uneven_shapes_with_graph(ctx):
     batch.sweep(1, 4, 2, graph=True)
     for a, b in zip(alone, mixed):
         assert np.array_equal(a.get_image(), b.get_image())
+
+
+@pytest.mark.parametrize("case", ALL, ids=_ids)
+def test_link_trace_det_matches_oracle(ctx, case):
+    from sun_b200 import link_trace_det
+    N, dims, prec, lay = case
+    U, beta = _thermal(N, dims)
+    g = _make(ctx, N, dims, prec, lay, beta=beta)
+    g.Set(U)
+    t, d = link_trace_det(g)
+    ref = O.link_trace_det(g.Get(), list(dims))
+    assert np.abs(np.array([t.real, t.imag, d.real, d.imag]) - ref).max() < 1e-12
+
+
+def test_autotuner_caches_launch_shapes_and_keeps_results(tmp_path):
+    from sun_b200 import Context, Sweep, gauge
+    path = str(tmp_path / "tunecache.csv")
+    imgs = []
+    for tune in (False, True, True):  # untuned, tuned (search), tuned (from cache)
+        with Context(0, tune=tune, tune_cache_path=path if tune else None) as c:
+            g = gauge(c, N=3, dims=(8, 8, 8, 8), beta=6.0, atype=1, prec="f32", seed=5)
+            g.Init(hot=True)
+            Sweep(g, 1, 4, 2)
+            imgs.append(g.get_image())
+            g.Release()
+    lines = open(path).read().splitlines()
+    assert len(lines) == 2 and all(l.startswith("k_update N=3 f32") for l in lines)  # HB and OR, searched once
+    assert np.array_equal(imgs[0], imgs[1]) and np.array_equal(imgs[1], imgs[2])
+
+
+def test_allocation_failure_is_reported_and_server_retries(ctx):
+    from sun_b200 import Server, SunError, gauge, make_job
+    from sun_b200._native import lib
+    srv = Server(ctx, max_active=4)
+    try:
+        lib().sun_debug_fail_allocations(0)
+        with pytest.raises(SunError) as e:
+            gauge(ctx, N=3, dims=(4, 4, 4, 4), prec="f32")
+        assert e.value.status == 3  # SUN_ERR_OUT_OF_MEMORY
+        jid = srv.submit(make_job(N=3, dims=(4, 4, 4, 4), sweeps=2, seed=7))
+        assert srv.step() == [] and srv.pending() == (1, 0)  # admission deferred, job kept
+    finally:
+        lib().sun_debug_fail_allocations(-1)
+    res = []
+    for _ in range(5):
+        res += srv.step()
+    assert [r["id"] for r in res] == [jid] and res[0]["status"] == 0
+    srv.close()

@@ -231,3 +231,13 @@ def test_gauge_file_roundtrip(tmp_path, save_fp64):
     # precision mismatch is refused, like ReadBin_Gauge (io_gauge.cpp:736-737)
     rc, *_ = O.load_bin(3, X, f, save_fp64=not save_fp64)
     assert rc == -3
+
+
+def test_link_trace_det():
+    for N in (2, 3, 4, 6):
+        assert np.allclose(O.link_trace_det(O.cold(N, X44), X44), [1, 0, 1, 0])
+        U = O.hot(N, X44, 8)
+        t = O.link_trace_det(U, X44)
+        assert abs(t[2] - 1) < 1e-13 and abs(t[3]) < 1e-13
+        ref = np.trace(U.reshape(-1, N, N), axis1=1, axis2=2).mean() / N
+        assert abs(t[0] - ref.real) < 1e-14 and abs(t[1] - ref.imag) < 1e-14
