@@ -81,6 +81,13 @@ def _declare(L: C.CDLL) -> None:
     L.orc_save_bin.restype = C.c_int
     L.orc_load_bin.argtypes = [C.c_int, _ip, _dp, C.c_char_p, C.c_int, C.c_int, C.c_int, _ip, _dp]
     L.orc_load_bin.restype = C.c_int
+    L.orc_project_sun.argtypes = [C.c_int, _dp, _dp, C.c_int, C.c_double]
+    L.orc_exp_iq3.argtypes = [_dp, _dp]
+    L.orc_ape.argtypes = [C.c_int, _ip, _dp, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int]
+    L.orc_stout.argtypes = [_ip, _dp, C.c_double, C.c_int, C.c_int]
+    L.orc_hyp.argtypes = [C.c_int, _ip, _dp, C.POINTER(C.c_float), C.c_int, C.c_int, C.c_double, C.c_int]
+    L.orc_multihit.argtypes = [C.c_int, _ip, _dp, _dp, C.c_double, C.c_int, C.c_int, C.c_uint64]
+    L.orc_multihit_space.argtypes = [C.c_int, _ip, _dp, _dp, C.c_int]
 
 
 def _d(a: np.ndarray):
@@ -253,3 +260,51 @@ def load_bin(N, X, path, save_fp64=True, header_fp64=True, with_header=True):
     rc = lib().orc_load_bin(N, _dims(X), _d(U), path.encode(), int(save_fp64), int(header_fp64),
                             int(with_header), g, C.byref(b))
     return rc, U, list(g), b.value
+
+
+# -- smearing and multihit (src/smear/*.cu); dirmask bit mu selects direction mu
+SPACE, TIME = 7, 8
+
+
+def project_sun(W, Q, nhits, tol=0.0):
+    """Projection of Q onto SU(N) started from W (project_link / SU3project)."""
+    W = np.ascontiguousarray(W, dtype=np.complex128).copy()
+    Q = np.ascontiguousarray(Q, dtype=np.complex128)
+    lib().orc_project_sun(W.shape[-1], _d(W), _d(Q), nhits, tol)
+    return W
+
+
+def exp_iq3(Q):
+    Q = np.ascontiguousarray(Q, dtype=np.complex128)
+    E = np.zeros((3, 3), dtype=np.complex128)
+    lib().orc_exp_iq3(_d(Q), _d(E))
+    return E
+
+
+def ape(U, X, w, steps, nhits, tol, dirmask):
+    """In place."""
+    lib().orc_ape(U.shape[-1], _dims(X), _d(U), w, steps, nhits, tol, dirmask)
+
+
+def stout(U, X, w, steps, dirmask):
+    """In place (SU(3))."""
+    assert U.shape[-1] == 3
+    lib().orc_stout(_dims(X), _d(U), w, steps, dirmask)
+
+
+def hyp(U, X, alpha, steps, nhits, tol, dirmask):
+    """In place; alpha = (alpha1, alpha2, alpha3), stored as FP32."""
+    a = (C.c_float * 3)(*[float(v) for v in alpha])
+    lib().orc_hyp(U.shape[-1], _dims(X), _d(U), a, steps, nhits, tol, dirmask)
+
+
+def multihit(U, X, beta, nhit, seed, mode=RNG_PHILOX64):
+    out = np.empty_like(U)
+    lib().orc_multihit(U.shape[-1], _dims(X), _d(U), _d(out), beta, nhit, mode, seed)
+    return out
+
+
+def multihit_space(U, X, nhit):
+    out = np.empty_like(U)
+    lib().orc_multihit_space(U.shape[-1], _dims(X), _d(U), _d(out), nhit)
+    return out

@@ -14,6 +14,9 @@
 //   ref_probe reunit    IN OUT nx ny nz nt beta
 //   ref_probe ensemble  nx ny nz nt beta seed ntherm nmeas
 //   ref_probe timing    nx ny nz nt beta sweeps {f32soa12|f64soa}
+//   ref_probe smear     IN OUT nx ny nz nt beta KIND ARGS
+//       KIND ape_space|ape_time w steps nhits tol;  stout_space|stout_time w steps
+//            hyp_space|hyp_time steps nhits tol a1 a2 a3;  multihit_space nhit
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -35,6 +38,7 @@
 #include <monte/ovr.h>
 #include <random.h>
 #include <reunitarize.h>
+#include <smear/smear.h>
 
 using namespace CULQCD;
 
@@ -179,6 +183,55 @@ static int cmd_timing(int argc, char** a)
     return 2;
 }
 
+// smearing through the reference API on a normal-order SOA copy (the only
+// order its smearing accepts); the result is written back in even/odd order
+template <class Real> static int cmd_smear(int argc, char** a)
+{
+    if (argc < 10) return 2;
+    setup(a, 4);
+    const std::string kind = a[9];
+    gauge AA(SOA, Device, PARAMS::Volume * 4, true);
+    ReadBin_Gauge<Real, double>(AA, a[2], true);
+    gauge BB(SOA, Device, PARAMS::Volume * 4, false);
+    BB.Copy(AA);
+    int rc = 0;
+    if ((kind == "ape_space" || kind == "ape_time") && argc >= 14) {
+        const Real w = atof(a[10]), tol = atof(a[13]);
+        const int steps = atoi(a[11]), nhits = atoi(a[12]);
+        if (kind == "ape_space") ApplyAPEinSpace<Real>(BB, w, steps, nhits, tol);
+        else ApplyAPEinTime<Real>(BB, w, steps, nhits, tol);
+    } else if ((kind == "stout_space" || kind == "stout_time") && argc >= 12) {
+        const Real w = atof(a[10]);
+        const int steps = atoi(a[11]);
+        if (kind == "stout_space") ApplyStoutinSpace<Real>(BB, w, steps);
+        else ApplyStoutinTime<Real>(BB, w, steps);
+    } else if ((kind == "hyp_space" || kind == "hyp_time") && argc >= 16) {
+        const int steps = atoi(a[10]), nhits = atoi(a[11]);
+        const Real tol = atof(a[12]);
+        ParamHYP hyp((float)atof(a[13]), (float)atof(a[14]), (float)atof(a[15]));
+        if (kind == "hyp_space") ApplyHYPinSpace<Real>(BB, steps, nhits, tol, hyp);
+        else ApplyHYPinTime<Real>(BB, steps, nhits, tol, hyp);
+    } else if (kind == "multihit_space" && argc >= 11) {
+        gauge CC(SOA, Device, PARAMS::Volume * 4, false);
+        CC.Copy(BB);
+        RNG rng;
+        rng.Init(1u);
+        ApplyMultiHitSpace<Real>(CC, BB, rng, atoi(a[10]));
+        rng.Release();
+        CC.Release();
+    } else {
+        rc = 2;
+    }
+    cudaDeviceSynchronize();
+    if (rc == 0) {
+        AA.Copy(BB);
+        SaveBin_Gauge<Real, double>(AA, a[3], true);
+    }
+    BB.Release();
+    AA.Release();
+    return rc;
+}
+
 int main(int argc, char** argv)
 {
     if (argc < 2) {
@@ -194,6 +247,7 @@ int main(int argc, char** argv)
     else if (c == "reunit") rc = cmd_reunit<double>(argc, argv);
     else if (c == "ensemble") rc = cmd_ensemble<double>(argc, argv);
     else if (c == "timing") rc = cmd_timing(argc, argv);
+    else if (c == "smear") rc = cmd_smear<double>(argc, argv);
     fflush(stdout);
     if (rc == 2) fprintf(stderr, "bad arguments\n");
     EndCULQCD(rc);

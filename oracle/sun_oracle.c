@@ -928,3 +928,6 @@ int orc_load_bin(int N, const int X[4], double *U, const char *path, int save_fp
     fclose(f);
     return ok ? 0 : -2;
 }
+
+/* smearing and multihit share this file's helpers */
+#include "sun_oracle_smear.inc"

@@ -97,6 +97,18 @@ int  orc_save_bin(int N, const int X[4], const double *U, double beta, const cha
 int  orc_load_bin(int N, const int X[4], double *U, const char *path, int save_fp64,
                   int header_fp64, int with_header, int grid_out[4], double *beta_out);
 
+/* --- smearing and multihit (sun_oracle_smear.inc) ---------------------------
+ * dirmask: bit mu selects direction mu (7 = space, 8 = time). */
+void orc_project_sun(int N, double *W, const double *Q, int nhits, double tol);
+void orc_exp_iq3(const double *Q, double *E);
+void orc_ape(int N, const int X[4], double *U, double w, int steps, int nhits, double tol, int dirmask);
+void orc_stout(const int X[4], double *U, double w, int steps, int dirmask);
+void orc_hyp(int N, const int X[4], double *U, const float alpha[3], int steps, int nhits, double tol,
+             int dirmask);
+void orc_multihit(int N, const int X[4], const double *Uin, double *Uout, double beta, int nhit,
+                  int mode, uint64_t seed);
+void orc_multihit_space(int N, const int X[4], const double *Uin, double *Uout, int nhit);
+
 #ifdef __cplusplus
 }
 #endif
