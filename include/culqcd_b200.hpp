@@ -232,6 +232,71 @@ template <class Real> void WilsonLoop(_gauge<Real>& array, _complex<Real>* res, 
     for (int i = 0; i < (R + 1) * (T + 1); ++i) res[i] = _complex<Real>((Real)o[2 * i], (Real)o[2 * i + 1]);
 }
 
+// smearing (include/smear/smear.h): in place on `array`, any layout and order
+template <class Real> void ApplyAPEinSpace(_gauge<Real> array, Real w, int steps, int nhits, Real tol)
+{
+    detail::check(sun_smear_ape(array.lat(), w, steps, nhits, tol, SUN_SMEAR_SPACE, nullptr), "ApplyAPEinSpace");
+}
+template <class Real> void ApplyAPEinTime(_gauge<Real> array, Real w, int steps, int nhits, Real tol)
+{
+    detail::check(sun_smear_ape(array.lat(), w, steps, nhits, tol, SUN_SMEAR_TIME, nullptr), "ApplyAPEinTime");
+}
+template <class Real> void ApplyStoutinSpace(_gauge<Real> array, Real w, int steps)
+{
+    detail::check(sun_smear_stout(array.lat(), w, steps, SUN_SMEAR_SPACE, nullptr), "ApplyStoutinSpace");
+}
+template <class Real> void ApplyStoutinTime(_gauge<Real> array, Real w, int steps)
+{
+    detail::check(sun_smear_stout(array.lat(), w, steps, SUN_SMEAR_TIME, nullptr), "ApplyStoutinTime");
+}
+
+// HYP weights (src/smear/hyp.cu:374-398); copyToGPUMem has nothing to do:
+// the weights travel with each call
+class ParamHYP {
+    float alpha1, alpha2, alpha3;
+
+public:
+    ParamHYP() { setDefault(); }
+    ParamHYP(float a1, float a2, float a3) { set(a1, a2, a3); }
+    void setDefault() { set(0.75f, 0.6f, 0.3f); }
+    void set(float a1, float a2, float a3)
+    {
+        alpha1 = a1;
+        alpha2 = a2;
+        alpha3 = a3;
+    }
+    void print() const { printf("HYP alpha1 = %g alpha2 = %g alpha3 = %g\n", alpha1, alpha2, alpha3); }
+    void copyToGPUMem() const {}
+    void get(double a[3]) const
+    {
+        a[0] = alpha1;
+        a[1] = alpha2;
+        a[2] = alpha3;
+    }
+};
+
+template <class Real> void ApplyHYPinSpace(_gauge<Real> array, int steps, int nhits, Real tol, ParamHYP hyp)
+{
+    double a[3];
+    hyp.get(a);
+    detail::check(sun_smear_hyp(array.lat(), a, steps, nhits, tol, SUN_SMEAR_SPACE, nullptr), "ApplyHYPinSpace");
+}
+template <class Real> void ApplyHYPinTime(_gauge<Real> array, int steps, int nhits, Real tol, ParamHYP hyp)
+{
+    double a[3];
+    hyp.get(a);
+    detail::check(sun_smear_hyp(array.lat(), a, steps, nhits, tol, SUN_SMEAR_TIME, nullptr), "ApplyHYPinTime");
+}
+// arrayout: SOA layout; the RNG's seed keys the Philox stream
+template <class Real> void ApplyMultiHit(_gauge<Real> array, _gauge<Real> arrayout, RNG& randstates, int nhit)
+{
+    detail::check(sun_multihit(array.lat(), arrayout.lat(), nhit, randstates.seed, nullptr), "ApplyMultiHit");
+}
+template <class Real> void ApplyMultiHitSpace(_gauge<Real> array, _gauge<Real> arrayout, RNG& /*randstates*/, int nhit)
+{
+    detail::check(sun_multihit_space(array.lat(), arrayout.lat(), nhit, nullptr), "ApplyMultiHitSpace");
+}
+
 template <class Real, class RealSave>
 void SaveBin_Gauge(_gauge<Real>& array, const std::string& file, bool withheader = false)
 {

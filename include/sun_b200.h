@@ -153,6 +153,41 @@ sun_status sun_plaquette_noalloc(const void *d_links, const sun_lattice_params *
 sun_status sun_polyakov(sun_lattice *lat, double out[2], void *stream);
 sun_status sun_wilson_loops(sun_lattice *lat, int R, int T, double *out, void *stream);
 
+/* ---- smearing and multihit (src/smear/) ----
+ * dirmask: bit mu selects direction mu; SUN_SMEAR_SPACE (x, y, z) is the
+ * reference's "...inSpace", SUN_SMEAR_TIME its "...inTime".  Each step
+ * rebuilds the selected directions from the unchanged field, in place.  Any
+ * layout and storage order is accepted (the reference takes normal-order SOA
+ * only).  Projections onto SU(N) use Cabibbo-Marinari SU(2) hits:
+ * project_link (include/projectlink.h:17) from the unsmeared link, stopping
+ * at relative change <= tol, or for SU(3) APE SU3project (projectlink.h:119)
+ * from the unit matrix with nhits hits. */
+#define SUN_SMEAR_SPACE 7
+#define SUN_SMEAR_TIME 8
+/* ApplyAPEinSpace / ApplyAPEinTime (src/smear/ape.cu:192, :237):
+ * U' = P[(U + w S) / (1 + 6 w)], S the staple over the spatial planes */
+sun_status sun_smear_ape(sun_lattice *lat, double w, int steps, int nhits, double tol, int dirmask,
+                         void *stream);
+/* ApplyStoutinSpace / ApplyStoutinTime (src/smear/stout.cu:687, :734), SU(3)
+ * only (SUN_ERR_UNSUPPORTED otherwise): U' = exp(iQ) U, Q the traceless
+ * Hermitian part of -i (w S) U^dagger */
+sun_status sun_smear_stout(sun_lattice *lat, double w, int steps, int dirmask, void *stream);
+/* ApplyHYPinSpace / ApplyHYPinTime (src/smear/hyp.cu:277, :328) with
+ * ParamHYP alpha = {alpha1, alpha2, alpha3} (reference default 0.75, 0.6,
+ * 0.3), used as FP32 like the reference's constants */
+sun_status sun_smear_hyp(sun_lattice *lat, const double alpha[3], int steps, int nhits, double tol, int dirmask,
+                         void *stream);
+/* ApplyMultiHit (src/smear/multihit.cu:318): dst <- src, then each temporal
+ * link of dst is the mean of the link and nhit heatbath updates of it against
+ * its staple in src (beta of src).  dst: same N, geometry, precision and
+ * order as src, SOA layout.  Random numbers: the Philox stream of link
+ * (lex, 3) with purpose 2 under `seed` (the reference's RNG& argument). */
+sun_status sun_multihit(sun_lattice *src, sun_lattice *dst, int nhit, uint64_t seed, void *stream);
+/* ApplyMultiHitSpace (src/smear/multihitsp.cu:246): dst <- src, then each
+ * spatial link of dst is the mean of nhit overrelaxation iterates of it
+ * against its spatial staple in src; nhit >= 1 */
+sun_status sun_multihit_space(sun_lattice *src, sun_lattice *dst, int nhit, void *stream);
+
 /* ---- gauge file: SaveBin_Gauge<Real,RealSave> / ReadBin_Gauge
  * (src/io_gauge.cpp:429, :605), byte-compatible; save_fp64 selects RealSave,
  * the header's beta field has the lattice's own precision ---- */

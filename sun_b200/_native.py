@@ -77,6 +77,11 @@ _SIGS = {
     "sun_plaquette_noalloc": [_vp, C.POINTER(SunLatticeParams), _vp, _vp],
     "sun_polyakov": [_vp, _dp, _vp],
     "sun_wilson_loops": [_vp, C.c_int, C.c_int, _dp, _vp],
+    "sun_smear_ape": [_vp, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, _vp],
+    "sun_smear_stout": [_vp, C.c_double, C.c_int, C.c_int, _vp],
+    "sun_smear_hyp": [_vp, _dp, C.c_int, C.c_int, C.c_double, C.c_int, _vp],
+    "sun_multihit": [_vp, _vp, C.c_int, C.c_uint64, _vp],
+    "sun_multihit_space": [_vp, _vp, C.c_int, _vp],
     "sun_save_bin": [_vp, C.c_char_p, C.c_int, C.c_int],
     "sun_load_bin": [_vp, C.c_char_p, C.c_int, C.c_int],
     "sun_batch_create": [_vp, C.POINTER(_vp)],

@@ -246,6 +246,74 @@ def WilsonLoop(g: gauge, R: int, T: int) -> np.ndarray:
     return o[..., 0] + 1j * o[..., 1]
 
 
+# -- smearing and multihit (src/smear/); in place unless an output is given --
+SMEAR_SPACE, SMEAR_TIME = 7, 8
+
+
+def ApplyAPEinSpace(g: gauge, w: float, steps: int, nhits: int, tol: float) -> None:
+    """APE smearing of the spatial links (src/smear/ape.cu:192)."""
+    check(lib().sun_smear_ape(g.h, w, steps, nhits, tol, SMEAR_SPACE, None), g.ctx.h)
+
+
+def ApplyAPEinTime(g: gauge, w: float, steps: int, nhits: int, tol: float) -> None:
+    """APE smearing of the temporal links (src/smear/ape.cu:237)."""
+    check(lib().sun_smear_ape(g.h, w, steps, nhits, tol, SMEAR_TIME, None), g.ctx.h)
+
+
+def ApplyStoutinSpace(g: gauge, w: float, steps: int) -> None:
+    """Stout smearing of the spatial links, SU(3) (src/smear/stout.cu:687)."""
+    check(lib().sun_smear_stout(g.h, w, steps, SMEAR_SPACE, None), g.ctx.h)
+
+
+def ApplyStoutinTime(g: gauge, w: float, steps: int) -> None:
+    """Stout smearing of the temporal links, SU(3) (src/smear/stout.cu:734)."""
+    check(lib().sun_smear_stout(g.h, w, steps, SMEAR_TIME, None), g.ctx.h)
+
+
+class ParamHYP:
+    """HYP weights alpha1, alpha2, alpha3 (ParamHYP, src/smear/hyp.cu:374-398), FP32."""
+
+    def __init__(self, alpha1: float = 0.75, alpha2: float = 0.6, alpha3: float = 0.3):
+        self.set(alpha1, alpha2, alpha3)
+
+    def setDefault(self) -> None:
+        self.set(0.75, 0.6, 0.3)
+
+    def set(self, alpha1: float, alpha2: float, alpha3: float) -> None:
+        self.alpha = (float(np.float32(alpha1)), float(np.float32(alpha2)), float(np.float32(alpha3)))
+
+    def print(self) -> None:
+        print("HYP: alpha1 = %g alpha2 = %g alpha3 = %g" % self.alpha)
+
+
+def _hyp(g: gauge, steps: int, nhits: int, tol: float, hyp: Optional[ParamHYP], mask: int) -> None:
+    a = (C.c_double * 3)(*(hyp or ParamHYP()).alpha)
+    check(lib().sun_smear_hyp(g.h, a, steps, nhits, tol, mask, None), g.ctx.h)
+
+
+def ApplyHYPinSpace(g: gauge, steps: int, nhits: int, tol: float, hyp: Optional[ParamHYP] = None) -> None:
+    """HYP smearing of the spatial links (src/smear/hyp.cu:277)."""
+    _hyp(g, steps, nhits, tol, hyp, SMEAR_SPACE)
+
+
+def ApplyHYPinTime(g: gauge, steps: int, nhits: int, tol: float, hyp: Optional[ParamHYP] = None) -> None:
+    """HYP smearing of the temporal links (src/smear/hyp.cu:328)."""
+    _hyp(g, steps, nhits, tol, hyp, SMEAR_TIME)
+
+
+def ApplyMultiHit(g: gauge, out: gauge, seed: int, nhit: int) -> None:
+    """out <- g with each temporal link replaced by the mean of itself and nhit
+    heatbath updates against its staple (src/smear/multihit.cu:318).  `seed`
+    keys the Philox stream (the reference takes an RNG&); out uses SOA."""
+    check(lib().sun_multihit(g.h, out.h, nhit, seed, None), out.ctx.h)
+
+
+def ApplyMultiHitSpace(g: gauge, out: gauge, nhit: int) -> None:
+    """out <- g with each spatial link replaced by the mean of nhit
+    overrelaxation iterates (src/smear/multihitsp.cu:246); out uses SOA."""
+    check(lib().sun_multihit_space(g.h, out.h, nhit, None), out.ctx.h)
+
+
 def SaveBin_Gauge(g: gauge, filename: str, withheader: bool = True, save_fp64: bool = True) -> None:
     check(lib().sun_save_bin(g.h, filename.encode(), int(save_fp64), int(withheader)), g.ctx.h)
 

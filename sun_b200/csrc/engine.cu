@@ -769,30 +769,40 @@ sun_status sun_lattice_download(sun_lattice* l, void* host, sun_host_format fmt,
     });
 }
 
+extern "C++" {
+namespace {
+
+// dst <- src through the canonical FP64 order (layout, order and precision
+// conversion); the RNG counters travel with the links
+void copy_links(sun_lattice* dst, sun_lattice* src, cudaStream_t s)
+{
+    if (dst->p.ncolors != src->p.ncolors) fail(SUN_ERR_INVALID_ARG, "copy between different N");
+    for (int k = 0; k < 4; ++k)
+        if (dst->p.dims[k] != src->p.dims[k]) fail(SUN_ERR_INVALID_ARG, "copy between different geometries");
+    const size_t V = src->desc.V, N = src->p.ncolors;
+    DevBuf stage;
+    stage.ensure(V * 4 * N * N * 16);
+    {
+        Solo so(src);
+        BatchView v = so.g.view(WORK_LINKS, src->ctx->blk_links, s);
+        OPS_CALL(src->p.ncolors, unpack, so.g.fp64, so.g.layout, v, src->ctx->blk_links, stage.p, s);
+    }
+    {
+        Solo so(dst);
+        BatchView v = so.g.view(WORK_LINKS, dst->ctx->blk_links, s);
+        OPS_CALL(dst->p.ncolors, pack, so.g.fp64, so.g.layout, v, dst->ctx->blk_links, stage.p, s);
+    }
+    ck(cudaMemcpyAsync(dst->state.p, src->state.p, 2 * sizeof(unsigned), cudaMemcpyDeviceToDevice, s), "copy");
+    ck(cudaStreamSynchronize(s), "copy");
+}
+
+}  // namespace
+}  // extern "C++"
+
 sun_status sun_lattice_copy(sun_lattice* dst, sun_lattice* src, void* stream)
 {
     if (!dst || !src) return SUN_ERR_INVALID_ARG;
-    return handle(dst->ctx, [&] {
-        if (dst->p.ncolors != src->p.ncolors) fail(SUN_ERR_INVALID_ARG, "copy between different N");
-        for (int k = 0; k < 4; ++k)
-            if (dst->p.dims[k] != src->p.dims[k]) fail(SUN_ERR_INVALID_ARG, "copy between different geometries");
-        cudaStream_t s = S(dst->ctx, stream);
-        const size_t V = src->desc.V, N = src->p.ncolors;
-        DevBuf stage;
-        stage.ensure(V * 4 * N * N * 16);
-        {
-            Solo so(src);
-            BatchView v = so.g.view(WORK_LINKS, src->ctx->blk_links, s);
-            OPS_CALL(src->p.ncolors, unpack, so.g.fp64, so.g.layout, v, src->ctx->blk_links, stage.p, s);
-        }
-        {
-            Solo so(dst);
-            BatchView v = so.g.view(WORK_LINKS, dst->ctx->blk_links, s);
-            OPS_CALL(dst->p.ncolors, pack, so.g.fp64, so.g.layout, v, dst->ctx->blk_links, stage.p, s);
-        }
-        ck(cudaMemcpyAsync(dst->state.p, src->state.p, 2 * sizeof(unsigned), cudaMemcpyDeviceToDevice, s), "copy");
-        ck(cudaStreamSynchronize(s), "copy");
-    });
+    return handle(dst->ctx, [&] { copy_links(dst, src, S(dst->ctx, stream)); });
 }
 
 sun_status sun_lattice_get_rng(sun_lattice* l, uint64_t* seed, uint32_t* hb, uint32_t* sw)
@@ -943,6 +953,125 @@ sun_status sun_wilson_loops(sun_lattice* l, int R, int T, double* out, void* str
         });
         const double norm = 3.0 * l->p.ncolors * (double)l->desc.V;
         for (int i = 0; i < nv; ++i) out[i] = r[i] / norm;
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Smearing (src/smear/*.cu).  Each step rebuilds the selected directions from
+// the unchanged field: the steps alternate between the lattice's image and a
+// scratch copy (the unselected directions are equal in both), and an odd
+// step count ends with one copy back.
+extern "C++" {
+namespace {
+
+constexpr int kSmearBlock = 128;  // the smearing kernels' __launch_bounds__
+
+void check_dirmask(int dirmask)
+{
+    if (dirmask <= 0 || dirmask > 15) fail(SUN_ERR_INVALID_ARG, "direction mask %d not in 1..15", dirmask);
+}
+
+template <class F> void smear_steps(sun_lattice* l, int steps, cudaStream_t s, F step)
+{
+    if (steps <= 0) return;
+    DevBuf tmp;
+    tmp.ensure(l->bytes);
+    ck(cudaMemcpyAsync(tmp.p, l->links.p, l->bytes, cudaMemcpyDeviceToDevice, s), "smear scratch");
+    Solo so(l);
+    BatchView v = so.g.view(WORK_SITES, kSmearBlock, s);
+    void* img[2] = {l->links.p, tmp.p};
+    for (int st = 0; st < steps; ++st) step(so.g, v, img[st & 1], img[(st + 1) & 1]);
+    if (steps & 1) ck(cudaMemcpyAsync(l->links.p, tmp.p, l->bytes, cudaMemcpyDeviceToDevice, s), "smear copy");
+    ck(cudaStreamSynchronize(s), "smearing");
+}
+
+void check_pair(sun_lattice* src, sun_lattice* dst)
+{
+    if (src == dst) fail(SUN_ERR_INVALID_ARG, "multihit needs distinct input and output lattices");
+    if (dst->p.ncolors != src->p.ncolors || dst->p.precision != src->p.precision || dst->p.order != src->p.order)
+        fail(SUN_ERR_INVALID_ARG, "multihit input and output differ in N, precision or order");
+    for (int k = 0; k < 4; ++k)
+        if (dst->p.dims[k] != src->p.dims[k]) fail(SUN_ERR_INVALID_ARG, "multihit geometries differ");
+    if (dst->p.layout != SUN_SOA) fail(SUN_ERR_INVALID_ARG, "multihit output must use the SOA layout (averages are not SU(N))");
+}
+
+}  // namespace
+}  // extern "C++"
+
+sun_status sun_smear_ape(sun_lattice* l, double w, int steps, int nhits, double tol, int dirmask, void* stream)
+{
+    if (!l || steps < 0 || nhits < 0) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        check_dirmask(dirmask);
+        cudaStream_t s = S(l->ctx, stream);
+        smear_steps(l, steps, s, [&](Group& g, const BatchView& v, const void* src, void* dst) {
+            OPS_CALL(g.N, ape, g.fp64, g.layout, v, kSmearBlock, src, dst, dirmask, w, nhits, tol, s);
+        });
+    });
+}
+
+sun_status sun_smear_stout(sun_lattice* l, double w, int steps, int dirmask, void* stream)
+{
+    if (!l || steps < 0) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        check_dirmask(dirmask);
+        if (l->p.ncolors != 3) fail(SUN_ERR_UNSUPPORTED, "stout smearing is defined for SU(3) only");
+        cudaStream_t s = S(l->ctx, stream);
+        smear_steps(l, steps, s, [&](Group& g, const BatchView& v, const void* src, void* dst) {
+            OPS_CALL(g.N, stout, g.fp64, g.layout, v, kSmearBlock, src, dst, dirmask, w, s);
+        });
+    });
+}
+
+sun_status sun_smear_hyp(sun_lattice* l, const double alpha[3], int steps, int nhits, double tol, int dirmask,
+                         void* stream)
+{
+    if (!l || !alpha || steps < 0 || nhits < 0) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        check_dirmask(dirmask);
+        cudaStream_t s = S(l->ctx, stream);
+        // the reference keeps the three weights as FP32 constants (constants.cu:424-463)
+        const double a1 = (float)alpha[0], a2 = (float)alpha[1], a3 = (float)alpha[2];
+        const size_t nn = (size_t)l->p.ncolors * l->p.ncolors;
+        const size_t slot_bytes = nn * (size_t)l->desc.V * (l->p.precision == SUN_F64 ? 16 : 8);
+        DevBuf b1, b2;
+        b1.ensure(16 * slot_bytes);
+        b2.ensure(16 * slot_bytes);
+        smear_steps(l, steps, s, [&](Group& g, const BatchView& v, const void* src, void* dst) {
+            OPS_CALL(g.N, hyp, g.fp64, g.layout, v, kSmearBlock, 1, src, b1.p, b2.p, dst, dirmask, a3, nhits, tol, s);
+            OPS_CALL(g.N, hyp, g.fp64, g.layout, v, kSmearBlock, 2, src, b1.p, b2.p, dst, dirmask, a2, nhits, tol, s);
+            OPS_CALL(g.N, hyp, g.fp64, g.layout, v, kSmearBlock, 3, src, b1.p, b2.p, dst, dirmask, a1, nhits, tol, s);
+        });
+    });
+}
+
+sun_status sun_multihit(sun_lattice* src, sun_lattice* dst, int nhit, uint64_t seed, void* stream)
+{
+    if (!src || !dst || nhit < 0) return SUN_ERR_INVALID_ARG;
+    return handle(dst->ctx, [&] {
+        check_pair(src, dst);
+        cudaStream_t s = S(dst->ctx, stream);
+        copy_links(dst, src, s);
+        Solo so(src);
+        BatchView v = so.g.view(WORK_SITES, kSmearBlock, s);
+        OPS_CALL(src->p.ncolors, multihit, so.g.fp64, so.g.layout, v, kSmearBlock, src->links.p, dst->links.p, nhit,
+                 (unsigned long long)seed, 0, s);
+        ck(cudaStreamSynchronize(s), "multihit");
+    });
+}
+
+sun_status sun_multihit_space(sun_lattice* src, sun_lattice* dst, int nhit, void* stream)
+{
+    if (!src || !dst || nhit <= 0) return SUN_ERR_INVALID_ARG;
+    return handle(dst->ctx, [&] {
+        check_pair(src, dst);
+        cudaStream_t s = S(dst->ctx, stream);
+        copy_links(dst, src, s);
+        Solo so(src);
+        BatchView v = so.g.view(WORK_SITES, kSmearBlock, s);
+        OPS_CALL(src->p.ncolors, multihit, so.g.fp64, so.g.layout, v, kSmearBlock, src->links.p, dst->links.p, nhit,
+                 0ull, 1, s);
+        ck(cudaStreamSynchronize(s), "multihit");
     });
 }
 

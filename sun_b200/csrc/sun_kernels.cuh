@@ -763,3 +763,5 @@ cudaError_t Ops<N>::unpack(int fp64, int layout, const BatchView& bv, int block,
 }
 
 }  // namespace sunb
+
+#include "sun_smear.cuh"

@@ -70,6 +70,21 @@ template <int N> struct Ops {
                             cudaStream_t s);
     static cudaError_t unpack(int fp64, int layout, const BatchView& bv, int block, void* canon,
                               cudaStream_t s);
+    // smearing: src and dst are distinct device images of the lattice, the
+    // launch rows are the directions in dirmask (bit mu selects mu)
+    static cudaError_t ape(int fp64, int layout, const BatchView& bv, int block, const void* src, void* dst,
+                           int dirmask, double w, int nhits, double tol, cudaStream_t s);
+    static cudaError_t stout(int fp64, int layout, const BatchView& bv, int block, const void* src, void* dst,
+                             int dirmask, double w, cudaStream_t s);
+    // HYP level 1 (alpha = alpha3), 2 (alpha2) or 3 (alpha1); b1, b2 hold 16
+    // N x N slots per site
+    static cudaError_t hyp(int fp64, int layout, const BatchView& bv, int block, int level, const void* src,
+                           void* b1, void* b2, void* dst, int dirmask, double alpha, int nhits, double tol,
+                           cudaStream_t s);
+    // heatbath multihit of the temporal links (space = 0) or overrelaxation
+    // multihit of the spatial links (space = 1); dst has the SOA layout
+    static cudaError_t multihit(int fp64, int layout, const BatchView& bv, int block, const void* src, void* dst,
+                                int nhit, unsigned long long seed, int space, cudaStream_t s);
 };
 
 extern template struct Ops<2>;

@@ -1,6 +1,7 @@
 // A CULQCD-style program (the reference's entry points and spelling) built
 // against include/culqcd_b200.hpp and libsun_b200.so: hot start, three sweeps
-// of 1 heatbath + 4 overrelaxation, reunitarization, measurements, save.
+// of 1 heatbath + 4 overrelaxation, reunitarization, measurements, save,
+// then APE smearing and multihit before a second Wilson loop.
 // usage: culqcd_demo OUTFILE
 #include <cstdio>
 
@@ -35,6 +36,15 @@ template <class Real> int run(const char* out)
     printf("polyakov %.17g %.17g\n", (double)l.real(), (double)l.imag());
     printf("wilson11 %.17g %.17g\n", (double)res[1 * 4 + 1].real(), (double)res[1 * 4 + 1].imag());
     SaveBin_Gauge<Real, double>(AA, out, true);
+    // the driver's smearing before Wilson loops (test.cpp:179-219): APE in
+    // space, then multihit of the temporal links into BB
+    ApplyAPEinSpace<Real>(BB, 0.2, 3, 10, 1.e-10);
+    gauge DD(SOA, Device, PARAMS::Volume * 4, false);
+    DD.Copy(BB);
+    ApplyMultiHit<Real>(DD, BB, rng, 5);
+    DD.Release();
+    WilsonLoop<Real>(BB, res, 2, 3);
+    printf("wilson11_smeared %.17g %.17g\n", (double)res[1 * 4 + 1].real(), (double)res[1 * 4 + 1].imag());
     BB.Release();
     AA.Release();
     return 0;

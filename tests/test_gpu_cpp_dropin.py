@@ -24,7 +24,7 @@ def test_culqcd_program_matches_python_api(ctx, tmp_path):
     out = subprocess.run([exe, f_cpp], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr
     vals = {l.split()[0]: [float(v) for v in l.split()[1:]] for l in out.stdout.splitlines()
-            if l.split() and l.split()[0] in ("plaquette", "polyakov", "wilson11")}
+            if l.split() and l.split()[0] in ("plaquette", "polyakov", "wilson11", "wilson11_smeared")}
 
     from sun_b200 import (SOA12, HeatBath, OnePolyakovLoop, OverRelaxation, PlaquetteCUB, Reunitarize,
                           SaveBin_Gauge, gauge)
@@ -48,3 +48,16 @@ def test_culqcd_program_matches_python_api(ctx, tmp_path):
     assert abs(vals["polyakov"][0] - l.real) < 1e-6
     w = O.wilson_loops(U, [4, 4, 4, 8], 2, 3)
     assert abs(vals["wilson11"][0] - w[1, 1, 0]) < 1e-6
+
+    # the same smearing through the Python API on a normal-order SOA copy
+    from sun_b200 import SOA, ApplyAPEinSpace, ApplyMultiHit, WilsonLoop
+    bb = gauge(ctx, N=3, dims=(4, 4, 4, 8), beta=6.0, atype=SOA, evenodd=False, prec="f32", seed=1234)
+    bb.Copy(g)
+    ApplyAPEinSpace(bb, 0.2, 3, 10, 1e-10)
+    dd = gauge(ctx, N=3, dims=(4, 4, 4, 8), beta=6.0, atype=SOA, evenodd=False, prec="f32", seed=1234)
+    dd.Copy(bb)
+    ApplyMultiHit(dd, bb, 1234, 5)
+    ws = WilsonLoop(bb, 2, 3)
+    # the C++ side returns the loop as _complex<float>: rounding of the result only
+    assert abs(vals["wilson11_smeared"][0] - ws[1, 1].real) < 1e-6
+    assert abs(vals["wilson11_smeared"][0] - vals["wilson11"][0]) > 1e-3
