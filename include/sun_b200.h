@@ -100,6 +100,14 @@ sun_status sun_lattice_init_hot(sun_lattice *lat, void *stream);
 /* host <-> device (gauge::Copy + cudaMemcpy of the reference) */
 sun_status sun_lattice_upload(sun_lattice *lat, const void *host, sun_host_format fmt, void *stream);
 sun_status sun_lattice_download(sun_lattice *lat, void *host, sun_host_format fmt, void *stream);
+/* Raw-image transfers that return at once (no reference counterpart: the
+ * reference's gauge::Copy is synchronous).  The copy is queued on `stream`
+ * and nothing waits for it; `host_image` (SUN_HOST_IMAGE format, sun_lattice_bytes
+ * long) must be page-locked for the copy to overlap other work, and must stay
+ * valid and untouched until the stream has passed the copy.  Order copies
+ * against sweeps on other streams with events. */
+sun_status sun_lattice_upload_async(sun_lattice *lat, const void *host_image, void *stream);
+sun_status sun_lattice_download_async(sun_lattice *lat, void *host_image, void *stream);
 /* layout / order / precision conversion, gauge::Copy (src/gaugearray.cu:130) */
 sun_status sun_lattice_copy(sun_lattice *dst, sun_lattice *src, void *stream);
 /* RNG state for checkpoint: RNG::Save / RNG::Read (src/random.cu:164, :183);

@@ -63,6 +63,8 @@ _SIGS = {
     "sun_lattice_upload": [_vp, _vp, C.c_int, _vp],
     "sun_lattice_download": [_vp, _vp, C.c_int, _vp],
     "sun_lattice_copy": [_vp, _vp, _vp],
+    "sun_lattice_upload_async": [_vp, _vp, _vp],
+    "sun_lattice_download_async": [_vp, _vp, _vp],
     "sun_lattice_get_rng": [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
     "sun_lattice_set_rng": [_vp, C.c_uint64, C.c_uint32, C.c_uint32],
     "sun_heatbath": [_vp, C.c_int, _vp],

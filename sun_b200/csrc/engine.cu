@@ -769,6 +769,22 @@ sun_status sun_lattice_download(sun_lattice* l, void* host, sun_host_format fmt,
     });
 }
 
+sun_status sun_lattice_upload_async(sun_lattice* l, const void* host_image, void* stream)
+{
+    if (!l || !host_image) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        ck(cudaMemcpyAsync(l->links.p, host_image, l->bytes, cudaMemcpyHostToDevice, S(l->ctx, stream)), "upload");
+    });
+}
+
+sun_status sun_lattice_download_async(sun_lattice* l, void* host_image, void* stream)
+{
+    if (!l || !host_image) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        ck(cudaMemcpyAsync(host_image, l->links.p, l->bytes, cudaMemcpyDeviceToHost, S(l->ctx, stream)), "download");
+    });
+}
+
 extern "C++" {
 namespace {
 
