@@ -351,6 +351,8 @@ def main():
                                     "hbm_gbs_model": 20 * V * k64 * 9 * 144 / t64 / 1e9}
         g64.Release()
         extras["batched"] = batched_bench(ctx, L, sp, stream, args)
+        extras["plain_small_fp64"] = plain_small_bench(ctx, L, sp, stream)
+        extras["sun_n"] = sun_n_bench(ctx, L, sp, stream)
         if rank == 0:
             extras["serving"] = serving_bench(ctx)
 
@@ -499,6 +501,81 @@ def batched_bench(ctx, L, sp, stream, args):
     b.close()
     for g in lats:
         g.Release()
+    return out
+
+
+def plain_small_bench(ctx, L, sp, stream, sweeps=200):
+    """The plain small case: SU(3) 8^4, beta = 6.0, cold start, FP64 full
+    links, even/odd, `sweeps` sweeps of 1 HB + 4 OR with the plaquette and the
+    Polyakov loop read back to the host after every sweep (the reference's
+    PlaquetteCUB / OnePolyakovLoop return host values).  The events bracket
+    the whole loop, host round trips included."""
+    import torch
+    from sun_b200 import gauge
+    from sun_b200._native import check
+    dims = (8, 8, 8, 8)
+    V = 8 ** 4
+    g = gauge(ctx, N=3, dims=dims, beta=6.0, atype=0, evenodd=True, prec="f64", seed=SEED)
+    g.Init(hot=False)
+    pl, po = (C.c_double * 2)(), (C.c_double * 2)()
+
+    def one():
+        check(L.sun_sweep(g.h, 1, 4, 1, sp), ctx.h)
+        check(L.sun_plaquette(g.h, pl, sp), ctx.h)
+        check(L.sun_polyakov(g.h, po, sp), ctx.h)
+
+    for _ in range(3):
+        one()
+    g.Init(hot=False)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(sweeps):
+        one()
+    e1.record(stream)
+    stream.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    out = {"value": 20 * V * sweeps / t, "unit": "link-updates/s", "sweeps": sweeps, "ms_per_sweep": 1e3 * t / sweeps,
+           "lattice": list(dims), "precision": "f64", "layout": "SOA", "start": "cold",
+           "final_plaquette": [pl[0], pl[1]], "final_polyakov": [po[0], po[1]],
+           "measure": "plaquette + Polyakov loop to the host every sweep"}
+    g.Release()
+    return out
+
+
+def sun_n_bench(ctx, L, sp, stream, sweeps=10):
+    """SU(N), N in {2, 4, 6}, on 24^4 with beta/(2 N^2) fixed (2.5, 11.1,
+    25.0): FP32 full links, FP64 compensated reductions, hot start; a bounded
+    sample of `sweeps` timed sweeps of 1 HB + 4 OR after 2 warm-up sweeps, then
+    the plaquette and Wilson loops R x T <= 4 x 4 of the final configuration."""
+    import torch
+    from sun_b200 import WilsonLoop, gauge
+    from sun_b200._native import check
+    peak, _ = measured_hbm()
+    dims = (24, 24, 24, 24)
+    V = 24 ** 4
+    out = {}
+    for n, beta in ((2, 2.5), (4, 11.1), (6, 25.0)):
+        g = gauge(ctx, N=n, dims=dims, beta=beta, atype=0, evenodd=True, prec="f32", seed=SEED + n, reunit_every=10)
+        g.Init(hot=True)
+        check(L.sun_sweep(g.h, 1, 4, 2, sp), ctx.h)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        check(L.sun_sweep(g.h, 1, 4, sweeps, sp), ctx.h)
+        e1.record(stream)
+        stream.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        rate = 20 * V * sweeps / t
+        pl = (C.c_double * 2)()
+        check(L.sun_plaquette(g.h, pl, sp), ctx.h)
+        w = WilsonLoop(g, 4, 4)
+        out[f"su{n}"] = {"value": rate, "unit": "link-updates/s", "beta": beta, "sweeps": sweeps,
+                         "hbm_frac": rate * 9 * 8 * n * n / 1e9 / peak, "plaquette": [pl[0], pl[1]],
+                         "wilson_4x4_re": [[round(float(v), 8) for v in row] for row in w.real]}
+        g.Release()
+    out["lattice"] = list(dims)
+    out["bytes_per_update"] = "9 link-records of 8 N^2 B (FP32 full links)"
     return out
 
 
