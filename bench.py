@@ -461,9 +461,18 @@ def serving_bench(ctx, rate=50.0, window=3.0, max_active=256):
     ok = [r for r in results if r["status"] == 0]
     lat = np.array([r["finish_s"] - r["submit_s"] for r in ok])
     upd = sum(r["link_updates"] for r in ok)
-    return {"jobs": len(jobs), "completed": len(ok), "arrival_rate_per_s": rate, "window_s": window,
-            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
-            "link_updates_per_s": upd / wall, "wall_s": wall, "max_active": max_active}
+    out = {"jobs": len(jobs), "completed": len(ok), "arrival_rate_per_s": rate, "window_s": window,
+           "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+           "link_updates_per_s": upd / wall, "wall_s": wall, "max_active": max_active}
+    if len(ok) == len(jobs):
+        # compulsory bytes: 9 link-records per update (48 B SU(3) 12-parameter,
+        # 8 N^2 B full FP32 links)
+        byts = sum(20 * int(np.prod(j["dims"])) * j["sweeps"] * 9 * (48 if j["N"] == 3 else 8 * j["N"] ** 2)
+                   for j in jobs)
+        peak, _ = measured_hbm()
+        out["hbm_gbs_model"] = byts / wall / 1e9
+        out["hbm_frac"] = byts / wall / 1e9 / peak
+    return out
 
 
 def batched_bench(ctx, L, sp, stream, args):
