@@ -50,17 +50,19 @@ SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
 
 // ---------------------------------------------------------------------------
 // Register caps of the update kernel (CTAs of 128 threads that must fit on an
-// SM).  The update is latency-bound at the register-limited occupancy; for
-// SU(3) overrelaxation a cap of 80 registers (6 CTAs, 24 warps per SM) was
-// measured fastest on B200.
+// SM).  The update is latency-bound at the register-limited occupancy.
+// Measured fastest for SU(3) on B200: overrelaxation FP32 80 registers
+// (6 CTAs, 24 warps per SM; 64 registers is no faster), heatbath FP32 102
+// registers (5 CTAs, 2.5 % faster than uncapped), overrelaxation FP64 168
+// registers (3 CTAs, 2 % faster); the FP64 heatbath is fastest uncapped.
 #ifndef SUN_OCC_F32_OR
 #define SUN_OCC_F32_OR 6
 #endif
 #ifndef SUN_OCC_F32_HB
-#define SUN_OCC_F32_HB 1
+#define SUN_OCC_F32_HB 5
 #endif
 #ifndef SUN_OCC_F64_OR
-#define SUN_OCC_F64_OR 1
+#define SUN_OCC_F64_OR 3
 #endif
 #ifndef SUN_OCC_F64_HB
 #define SUN_OCC_F64_HB 1
