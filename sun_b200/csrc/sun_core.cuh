@@ -163,7 +163,9 @@ template <class R, class Stream> SUN_DEV void su2_heatbath_draw(R al, Stream& st
 
 // Cabibbo-Marinari pseudo-heatbath of U against the staple sum S (F = S^dag)
 // -- heatBathSUN (include/device_PHB_OVR.h:362-485).  SU(3) recomputes each
-// block from U and S; other N keep M = U S^dagger and update it with U.
+// block from U and S like the reference; N >= 4 does the same (the
+// reference keeps M = U S^dagger and updates it with U, which needs N^2 more
+// live complex numbers); N = 2 keeps M.
 template <int N, class R, class Stream>
 SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, Stream& st)
 {
@@ -186,6 +188,23 @@ SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, St
             if (b == 0) su2_apply<N, R>(U, 0, 1, c);
             else if (b == 1) su2_apply<N, R>(U, 1, 2, c);
             else su2_apply<N, R>(U, 0, 2, c);
+        }
+    } else if constexpr (N >= 4) {
+        // each block of U S^dagger recomputed from U and S instead of
+        // keeping M = U S^dagger (N^2 fewer live complex numbers, no N^3
+        // product up front; the same values up to rounding), one rolled copy
+        // of the draw
+#pragma unroll 1
+        for (int b = 0; b < SubGroup<N>::count; ++b) {
+            R r[4], a[4], c[4];
+            with_subgroup<N>(b, [&](auto P, auto Q) { su2_block_US<N, R>(U, S, P(), Q(), r); });
+            R k = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+            R ap = beta_over_n * k;
+            k = R(1) / k;
+            r[0] *= k; r[1] *= k; r[2] *= k; r[3] *= k;
+            su2_heatbath_draw<R>(ap, st, a);
+            su2_mul_udag(a, r, c);
+            with_subgroup<N>(b, [&](auto P, auto Q) { su2_apply<N, R>(U, P(), Q(), c); });
         }
     } else {
         Mat<N, R> M;
@@ -226,10 +245,12 @@ template <class R> SUN_DEV void su2_overrelax_element(const R r[4], R c[4])
 
 template <int N, class R> SUN_DEV void overrelax_update(Mat<N, R>& U, const Mat<N, R>& S)
 {
-    if constexpr (N == 3) {
+    if constexpr (N >= 3) {
+        // blocks recomputed from U and S (for N >= 4 instead of the
+        // reference's M = U S^dagger: the same values up to rounding)
 #pragma unroll
-        for (int b = 0; b < 3; ++b) {
-            const int p = SubGroup<3>::p(b), q = SubGroup<3>::q(b);
+        for (int b = 0; b < SubGroup<N>::count; ++b) {
+            const int p = SubGroup<N>::p(b), q = SubGroup<N>::q(b);
             R r[4], c[4];
             su2_block_US<N, R>(U, S, p, q, r);
             su2_overrelax_element(r, c);

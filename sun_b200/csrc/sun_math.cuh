@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #define SUN_DEV __device__ __forceinline__
 #define SUN_HD __host__ __device__ __forceinline__
 
@@ -200,6 +202,19 @@ template <int N> struct SubGroup {
         return -1;
     }
 };
+
+// Calls f(P, Q) with the (p, q) of subgroup b as compile-time constants
+// (std::integral_constant), so the code in f indexes matrices statically,
+// i.e. keeps them in registers, although b is a runtime loop index.
+template <int N, int B = 0, class F> SUN_DEV void with_subgroup(int b, F&& f)
+{
+    if constexpr (B < SubGroup<N>::count) {
+        if (b == B)
+            f(std::integral_constant<int, SubGroup<N>::p(B)>{}, std::integral_constant<int, SubGroup<N>::q(B)>{});
+        else
+            with_subgroup<N, B + 1>(b, f);
+    }
+}
 
 // Block 4-vector of M restricted to rows/cols (p,q) -- get_block_su2
 // (include/device_PHB_OVR.h:265-272).
