@@ -353,6 +353,7 @@ def main():
         extras["batched"] = batched_bench(ctx, L, sp, stream, args)
         extras["plain_small_fp64"] = plain_small_bench(ctx, L, sp, stream)
         extras["sun_n"] = sun_n_bench(ctx, L, sp, stream)
+        extras["smearing"] = smear_bench(ctx, L, sp, stream)
         if rank == 0:
             extras["serving"] = serving_bench(ctx)
 
@@ -585,6 +586,48 @@ def sun_n_bench(ctx, L, sp, stream, sweeps=10):
         g.Release()
     out["lattice"] = list(dims)
     out["bytes_per_update"] = "9 link-records of 8 N^2 B (FP32 full links)"
+    return out
+
+
+def smear_bench(ctx, L, sp, stream):
+    """Smearing on SU(3) 24^4 (the step before Wilson loops): per layout, ms
+    per step of APE in space (w 0.2, 10 hits), stout in space (w 0.1), HYP
+    in space (alpha 0.75/0.6/0.3, 10 hits, tol 1e-10), the heatbath
+    multihit of the temporal links and the overrelaxation multihit of the
+    spatial links (10 hits each), each after one untimed call.  FP64 full
+    links in lexicographic order are the reference's smearing layout; FP32
+    12-parameter even/odd is the sweep's."""
+    import torch
+    from sun_b200 import gauge
+    from sun_b200._native import check
+    dims = (24, 24, 24, 24)
+    out = {"lattice": list(dims)}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    alpha = (C.c_double * 3)(0.75, 0.6, 0.3)
+
+    def timed(f, steps):
+        f(1)
+        stream.synchronize()
+        e0.record(stream)
+        f(steps)
+        e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    for name, lay, eo, prec in (("f64_soa_lex", 0, False, "f64"), ("f32_soa12_eo", 1, True, "f32")):
+        g = gauge(ctx, N=3, dims=dims, beta=6.0, atype=lay, evenodd=eo, prec=prec, seed=SEED)
+        g.Init(hot=True)
+        o = gauge(ctx, N=3, dims=dims, beta=6.0, atype=0, evenodd=eo, prec=prec, seed=SEED)
+        r = {}
+        r["ape_ms_per_step"] = timed(lambda n: check(L.sun_smear_ape(g.h, 0.2, n, 10, 1e-10, 7, sp), ctx.h), 3)
+        r["stout_ms_per_step"] = timed(lambda n: check(L.sun_smear_stout(g.h, 0.1, n, 7, sp), ctx.h), 3)
+        r["hyp_ms_per_step"] = timed(lambda n: check(L.sun_smear_hyp(g.h, alpha, n, 10, 1e-10, 7, sp), ctx.h), 1)
+        r["multihit_ms"] = timed(lambda n: [check(L.sun_multihit(g.h, o.h, 10, 99, sp), ctx.h) for _ in range(n)], 2)
+        r["multihit_space_ms"] = timed(lambda n: [check(L.sun_multihit_space(g.h, o.h, 10, sp), ctx.h)
+                                                  for _ in range(n)], 2)
+        out[name] = r
+        o.Release()
+        g.Release()
     return out
 
 

@@ -16,6 +16,7 @@
 //   ref_probe timing    nx ny nz nt beta sweeps {f32soa12|f64soa}
 //   ref_probe smear     IN OUT nx ny nz nt beta KIND ARGS
 //       KIND ape_space|ape_time w steps nhits tol;  stout_space|stout_time w steps
+//       (prints smear_ms: the smearing call's duration, CUDA events)
 //            hyp_space|hyp_time steps nhits tol a1 a2 a3;  multihit_space nhit
 #include <cuda_runtime.h>
 
@@ -195,6 +196,11 @@ template <class Real> static int cmd_smear(int argc, char** a)
     gauge BB(SOA, Device, PARAMS::Volume * 4, false);
     BB.Copy(AA);
     int rc = 0;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaDeviceSynchronize();
+    cudaEventRecord(t0, 0);
     if ((kind == "ape_space" || kind == "ape_time") && argc >= 14) {
         const Real w = atof(a[10]), tol = atof(a[13]);
         const int steps = atoi(a[11]), nhits = atoi(a[12]);
@@ -222,7 +228,11 @@ template <class Real> static int cmd_smear(int argc, char** a)
     } else {
         rc = 2;
     }
+    cudaEventRecord(t1, 0);
     cudaDeviceSynchronize();
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t0, t1);
+    printf("smear_ms %.6f\n", ms);
     if (rc == 0) {
         AA.Copy(BB);
         SaveBin_Gauge<Real, double>(AA, a[3], true);
