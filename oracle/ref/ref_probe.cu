@@ -14,6 +14,8 @@
 //   ref_probe reunit    IN OUT nx ny nz nt beta
 //   ref_probe ensemble  nx ny nz nt beta seed ntherm nmeas
 //   ref_probe timing    nx ny nz nt beta sweeps {f32soa12|f64soa}
+//   ref_probe plain     nx ny nz nt beta sweeps   (FP64 SOA, cold start, plaquette +
+//                       Polyakov loop every sweep; prints plain_ms)
 //   ref_probe smear     IN OUT nx ny nz nt beta KIND ARGS
 //       KIND ape_space|ape_time w steps nhits tol;  stout_space|stout_time w steps
 //       (prints smear_ms: the smearing call's duration, CUDA events)
@@ -175,6 +177,50 @@ template <class Real, ArrayType AT> static int run_timing(char** a)
     return 0;
 }
 
+// the plain small case: cold start, sweeps of 1 HeatBath + 4 OverRelaxation
+// with PlaquetteCUB and OnePolyakovLoop after every sweep, FP64 full links
+template <class Real> static int cmd_plain(int argc, char** a)
+{
+    if (argc < 8) return 2;
+    setup(a, 2);
+    const int sweeps = atoi(a[7]);
+    gauge AA(SOA, Device, PARAMS::Volume * 4, true);
+    AA.Init();
+    RNG rng;
+    rng.Init(1234u);
+    HeatBath<Real> hb(AA, rng);
+    OverRelaxation<Real> ovr(AA);
+    PlaquetteCUB<Real> plaq(AA);
+    OnePolyakovLoop<Real> poly(AA);
+    for (int w = 0; w < 3; ++w) {  // warm-up (and autotuning)
+        hb.Run();
+        ovr.Run();
+        plaq.Run();
+        poly.Run();
+    }
+    AA.Init();
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaDeviceSynchronize();
+    cudaEventRecord(e0, 0);
+    complexd p, l;
+    for (int s = 0; s < sweeps; ++s) {
+        hb.Run();
+        for (int k = 0; k < 4; ++k) ovr.Run();
+        p = plaq.Run();
+        l = poly.Run();
+    }
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    printf("plain_ms %.6f plaquette %.17g %.17g polyakov %.17g %.17g\n", ms, p.real(), p.imag(), l.real(), l.imag());
+    rng.Release();
+    AA.Release();
+    return 0;
+}
+
 static int cmd_timing(int argc, char** a)
 {
     if (argc < 9) return 2;
@@ -257,6 +303,7 @@ int main(int argc, char** argv)
     else if (c == "reunit") rc = cmd_reunit<double>(argc, argv);
     else if (c == "ensemble") rc = cmd_ensemble<double>(argc, argv);
     else if (c == "timing") rc = cmd_timing(argc, argv);
+    else if (c == "plain") rc = cmd_plain<double>(argc, argv);
     else if (c == "smear") rc = cmd_smear<double>(argc, argv);
     fflush(stdout);
     if (rc == 2) fprintf(stderr, "bad arguments\n");
