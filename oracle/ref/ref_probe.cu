@@ -14,6 +14,8 @@
 //   ref_probe reunit    IN OUT nx ny nz nt beta
 //   ref_probe ensemble  nx ny nz nt beta seed ntherm nmeas
 //   ref_probe timing    nx ny nz nt beta sweeps {f32soa12|f64soa}
+//   ref_probe batch     FILE sweeps  (lines 'L T beta': SU(3) L^3 x T lattices, FP32 SOA12,
+//                       one after another; prints batch_ms and link_updates)
 //   ref_probe plain     nx ny nz nt beta sweeps   (FP64 SOA, cold start, plaquette +
 //                       Polyakov loop every sweep; prints plain_ms)
 //   ref_probe smear     IN OUT nx ny nz nt beta KIND ARGS
@@ -177,6 +179,58 @@ template <class Real, ArrayType AT> static int run_timing(char** a)
     return 0;
 }
 
+// many lattices the reference's way, one after another (one process-global
+// geometry at a time): per lattice SETPARAMS, hot start, 3 untimed sweeps,
+// then `sweeps` timed sweeps of 1 HeatBath + 4 OverRelaxation with
+// Reunitarize every 10; the timed parts are summed
+template <class Real> static int cmd_batch(int argc, char** a)
+{
+    if (argc < 4) return 2;
+    FILE* f = fopen(a[2], "r");
+    if (!f) return 2;
+    const int sweeps = atoi(a[3]);
+    int l, t;
+    double beta;
+    double ms_total = 0, updates = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    unsigned seed = 1234;
+    while (fscanf(f, "%d %d %lf", &l, &t, &beta) == 3) {
+        PARAMS::UseTex = false;
+        SETPARAMS(false, beta, l, l, l, t, false);
+        gauge AA(SOA12, Device, PARAMS::Volume * 4, true);
+        RNG rng;
+        rng.Init(seed++);
+        AA.Init(rng);
+        HeatBath<Real> hb(AA, rng);
+        OverRelaxation<Real> ovr(AA);
+        Reunitarize<Real> reu(AA);
+        for (int w = 0; w < 3; ++w) {
+            hb.Run();
+            for (int k = 0; k < 4; ++k) ovr.Run();
+        }
+        cudaDeviceSynchronize();
+        cudaEventRecord(e0, 0);
+        for (int s = 0; s < sweeps; ++s) {
+            hb.Run();
+            for (int k = 0; k < 4; ++k) ovr.Run();
+            if ((s + 1) % 10 == 0) reu.Run();
+        }
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms_total += ms;
+        updates += 20.0 * PARAMS::Volume * sweeps;
+        rng.Release();
+        AA.Release();
+    }
+    fclose(f);
+    printf("batch_ms %.6f link_updates %.6e\n", ms_total, updates);
+    return 0;
+}
+
 // the plain small case: cold start, sweeps of 1 HeatBath + 4 OverRelaxation
 // with PlaquetteCUB and OnePolyakovLoop after every sweep, FP64 full links
 template <class Real> static int cmd_plain(int argc, char** a)
@@ -304,6 +358,7 @@ int main(int argc, char** argv)
     else if (c == "ensemble") rc = cmd_ensemble<double>(argc, argv);
     else if (c == "timing") rc = cmd_timing(argc, argv);
     else if (c == "plain") rc = cmd_plain<double>(argc, argv);
+    else if (c == "batch") rc = cmd_batch<float>(argc, argv);
     else if (c == "smear") rc = cmd_smear<double>(argc, argv);
     fflush(stdout);
     if (rc == 2) fprintf(stderr, "bad arguments\n");
