@@ -128,6 +128,17 @@ struct sun_ctx {
     size_t hbm_budget = 0;
     // launch shapes (CTA sizes) per kernel family
     int blk_update = 128, blk_sites = 128, blk_links = 256, blk_wilson = 64;
+    // update kernel: 0 chosen by size (or by the tuner), 1 always one thread
+    // per half-site (k_update), 2 always N lanes per half-site (k_update_rows).
+    // By size: groups of N >= 4, and of SU(3) with FP64 full links, with at
+    // most rows_max_halfv half-sites (FP64: half that) take the row-split
+    // kernel.  Sweeps measured on B200: SU(6) 8^4 FP32 3.1x and FP64 2.2x
+    // faster, 12^4 FP32 1.55x; SU(4) 8^4 16-21 %, 12^4 FP32 10 %; SU(3) FP64
+    // 8^4 5 %.  SU(2), SU(3) in FP32 and larger lattices are faster with one
+    // thread per half-site.
+    int upd_kernel = 0;
+    int blk_rows = 128;
+    long long rows_max_halfv = 16384;
     // autotuner (tuneLaunch, src/tune.cpp:304): CTA size of the update kernel
     // per (kernel class, total half-volume), timed once, cached in a CSV file
     bool tune = false;
@@ -238,27 +249,48 @@ struct Group {
     } while (0)
 
 // -- sweeps ------------------------------------------------------------------
-// CTA size of the update kernel for this group and mode.  With tuning on,
-// the first use of a (class, mode, total half-volume) key times one phase
-// launch per candidate size on the real lattices -- links backed up before and
-// restored after, like Tunable::preTune/postTune (include/tune.h:119,
-// monte.h:73-74) -- keeps the fastest and appends it to the cache file.
+// Launch shape of the update: cfg > 0 runs k_update with CTAs of cfg threads
+// (one per half-site), cfg < 0 runs k_update_rows with CTAs of -cfg threads
+// (N lanes per half-site, 32/N half-sites per warp).  Both give the same bits.
+int upd_sites_per_cta(int N, int cfg) { return cfg > 0 ? cfg : (-cfg / 32) * (32 / N); }
+
+BatchView upd_view(Group& g, int cfg, cudaStream_t s) { return g.view(WORK_HALF, upd_sites_per_cta(g.N, cfg), s); }
+
+void launch_update(Group& g, int mode, int cfg, const BatchView& v, int par, int mu, unsigned hb_offset,
+                   const InjView& inj, cudaStream_t s)
+{
+    if (cfg > 0) OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, cfg, par, mu, hb_offset, inj, s);
+    else OPS_CALL(g.N, update_rows, g.fp64, g.layout, mode, v, -cfg, par, mu, hb_offset, inj, s);
+}
+
+// Update launch shape for this group and mode.  Without tuning: by the size
+// rule of sun_ctx::upd_kernel.  With tuning on, the first use of a (class,
+// mode, total half-volume) key times one phase launch per candidate shape on
+// the real lattices -- links backed up before and restored after, like
+// Tunable::preTune/postTune (include/tune.h:119, monte.h:73-74) -- keeps the
+// fastest and appends it to the cache file.
 int update_block(sun_ctx* c, Group& g, int mode, cudaStream_t s)
 {
-    if (!c->tune) return c->blk_update;
     long long work = 0;
     size_t bytes = 0;
     for (auto* l : g.lats) {
         work += l->desc.halfV;
         bytes += l->bytes;
     }
+    const int fixed = c->upd_kernel == 1   ? c->blk_update
+                      : c->upd_kernel == 2 ? -c->blk_rows
+                      : (work <= (g.fp64 ? c->rows_max_halfv / 2 : c->rows_max_halfv) &&
+                                 (g.N >= 4 || (g.N == 3 && g.fp64 && g.layout == SUN_SOA))
+                             ? -c->blk_rows
+                             : c->blk_update);
+    if (!c->tune) return fixed;
     char key[160];
-    snprintf(key, sizeof key, "k_update N=%d %s layout=%d mode=%d halfV=%lld", g.N, g.fp64 ? "f64" : "f32", g.layout,
-             mode, work);
+    snprintf(key, sizeof key, "k_update N=%d %s layout=%d mode=%d halfV=%lld kernel=%d", g.N, g.fp64 ? "f64" : "f32",
+             g.layout, mode, work, c->upd_kernel);
     auto it = c->tuned.find(key);
     if (it != c->tuned.end()) return it->second;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return c->blk_update;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return fixed;
     DevBuf backup;
     backup.ensure(bytes);
     size_t off = 0;
@@ -270,13 +302,14 @@ int update_block(sun_ctx* c, Group& g, int mode, cudaStream_t s)
     ck(cudaEventCreate(&e0), "event");
     ck(cudaEventCreate(&e1), "event");
     InjView none{nullptr, 0, nullptr};
-    int best = c->blk_update;
+    int best = fixed;
     float best_ms = 1e30f;
-    for (int blk : {32, 64, 96, 128}) {
-        BatchView v = g.view(WORK_HALF, blk, s);
-        OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, blk, 0, 0, 0u, none, s);  // warm-up
+    for (int blk : {32, 64, 96, 128, -32, -64, -128}) {
+        if ((blk > 0 && c->upd_kernel == 2) || (blk < 0 && c->upd_kernel == 1)) continue;
+        BatchView v = upd_view(g, blk, s);
+        launch_update(g, mode, blk, v, 0, 0, 0u, none, s);  // warm-up
         ck(cudaEventRecord(e0, s), "event");
-        for (int r = 0; r < 3; ++r) OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, blk, 0, 0, 0u, none, s);
+        for (int r = 0; r < 3; ++r) launch_update(g, mode, blk, v, 0, 0, 0u, none, s);
         ck(cudaEventRecord(e1, s), "event");
         ck(cudaEventSynchronize(e1), "event");
         float ms = 0;
@@ -308,18 +341,22 @@ void group_sweep(sun_ctx* c, Group& g, int n_hb, int n_or, bool count_sweep, boo
 {
     if (g.lats.empty()) return;
     InjView none{nullptr, 0, nullptr};
-    const int bhb = n_hb > 0 ? update_block(c, g, MODE_HB, s) : c->blk_update;
-    const int bor = n_or > 0 ? update_block(c, g, MODE_OR, s) : c->blk_update;
-    BatchView vhb = g.view(WORK_HALF, bhb, s);
-    for (int h = 0; h < n_hb; ++h)
-        for (int par = 0; par < 2; ++par)
-            for (int mu = 0; mu < 4; ++mu)
-                OPS_CALL(g.N, update, g.fp64, g.layout, MODE_HB, vhb, bhb, par, mu, (unsigned)h, none, s);
-    BatchView vor = g.view(WORK_HALF, bor, s);
-    for (int o = 0; o < n_or; ++o)
-        for (int par = 0; par < 2; ++par)
-            for (int mu = 0; mu < 4; ++mu)
-                OPS_CALL(g.N, update, g.fp64, g.layout, MODE_OR, vor, bor, par, mu, 0u, none, s);
+    // a shape's table is made only for a mode that runs: inside a graph
+    // capture only the tables prepared before it exist
+    if (n_hb > 0) {
+        const int bhb = update_block(c, g, MODE_HB, s);
+        BatchView vhb = upd_view(g, bhb, s);
+        for (int h = 0; h < n_hb; ++h)
+            for (int par = 0; par < 2; ++par)
+                for (int mu = 0; mu < 4; ++mu) launch_update(g, MODE_HB, bhb, vhb, par, mu, (unsigned)h, none, s);
+    }
+    if (n_or > 0) {
+        const int bor = update_block(c, g, MODE_OR, s);
+        BatchView vor = upd_view(g, bor, s);
+        for (int o = 0; o < n_or; ++o)
+            for (int par = 0; par < 2; ++par)
+                for (int mu = 0; mu < 4; ++mu) launch_update(g, MODE_OR, bor, vor, par, mu, 0u, none, s);
+    }
     if (n_hb > 0 || count_sweep)
         ck(launch_end_sweep(reinterpret_cast<const LatDev*>(g.d_lats.p), (int)g.lats.size(), (unsigned)n_hb,
                             count_sweep ? 1u : 0u, s),
@@ -615,6 +652,15 @@ sun_status sun_init(const sun_config* cfg, sun_ctx** out)
         env_blk("SUN_B200_BLOCK_UPDATE", c->blk_update);
         env_blk("SUN_B200_BLOCK_SITES", c->blk_sites);
         env_blk("SUN_B200_BLOCK_LINKS", c->blk_links);
+        env_blk("SUN_B200_BLOCK_ROWS", c->blk_rows);
+        if (c->blk_rows > 128) c->blk_rows = 128;
+        // update kernel: "sites" (k_update), "rows" (k_update_rows) or
+        // "auto" (by size); SUN_B200_ROWS_MAX_HALFV moves the size threshold
+        if (const char* k = getenv("SUN_B200_UPDATE_KERNEL")) {
+            if (!strcmp(k, "sites")) c->upd_kernel = 1;
+            else if (!strcmp(k, "rows")) c->upd_kernel = 2;
+        }
+        if (const char* t = getenv("SUN_B200_ROWS_MAX_HALFV")) c->rows_max_halfv = atoll(t);
         *out = c.release();
     });
 }
@@ -878,13 +924,12 @@ sun_status sun_heatbath_injected(sun_lattice* l, const double* u, int stride, vo
         need_eo(l, "the heatbath update");
         cudaStream_t s = S(l->ctx, stream);
         Solo so(l);
-        BatchView half = so.g.view(WORK_HALF, l->ctx->blk_update, s);
+        const int cfg = update_block(l->ctx, so.g, MODE_HB, s);
+        BatchView half = upd_view(so.g, cfg, s);
         ck(cudaMemsetAsync(l->ctx->err.p, 0, sizeof(int), s), "memset");
         InjView inj{u, stride, reinterpret_cast<int*>(l->ctx->err.p)};
         for (int par = 0; par < 2; ++par)
-            for (int mu = 0; mu < 4; ++mu)
-                OPS_CALL(l->p.ncolors, update, so.g.fp64, so.g.layout, MODE_HB_INJECTED, half, l->ctx->blk_update,
-                         par, mu, 0u, inj, s);
+            for (int mu = 0; mu < 4; ++mu) launch_update(so.g, MODE_HB_INJECTED, cfg, half, par, mu, 0u, inj, s);
         int flag = 0;
         ck(cudaMemcpyAsync(&flag, l->ctx->err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "flag read");
         ck(cudaStreamSynchronize(s), "heatbath");
@@ -1278,8 +1323,8 @@ sun_status sun_batch_sweep(sun_batch* b, int n_hb, int n_or, int n_sweeps, int u
             for (auto& g : b->groups) {
                 if (g->lats.empty()) continue;
                 // launch shapes (tuned if tuning is on) and their tables, before capture
-                if (n_hb > 0) g->view(WORK_HALF, update_block(b->ctx, *g, MODE_HB, s), s);
-                if (n_or > 0) g->view(WORK_HALF, update_block(b->ctx, *g, MODE_OR, s), s);
+                if (n_hb > 0) upd_view(*g, update_block(b->ctx, *g, MODE_HB, s), s);
+                if (n_or > 0) upd_view(*g, update_block(b->ctx, *g, MODE_OR, s), s);
                 g->view(WORK_LINKS, b->ctx->blk_links, s);
             }
             cudaStream_t cs;

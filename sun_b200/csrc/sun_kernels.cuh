@@ -182,6 +182,155 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)
     IO::store(wbase, own, stride, U);
 }
 
+template <class R> SUN_DEV cx<R> shfl_cx(cx<R> v, int src)
+{
+    return mkc<R>(__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src));
+}
+
+// Row-split k_update for small lattices of larger N.  The N lanes of a site
+// (32/N sites per warp) each multiply out one row of every staple product,
+// the full neighbour links loaded by every lane (the repeats served by L1);
+// the lanes then exchange their rows of the staple sum by warp shuffles, all
+// run the same update on the same inputs, and lane 0 stores the link.  Per
+// lane this holds far fewer live values than one thread per site (SU(6)
+// FP32: no spills against 3.7 KB) and, on a lattice too small to fill the
+// GPU, shortens each site's chain of dependent instructions.  Every element
+// goes through the same operations in the same order as in k_update (the row
+// routines of sun_math.cuh), so both kernels give the same bits and either
+// may run any lattice.
+template <int N, class R, int LAYOUT, int MODE>
+__global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, int mu, unsigned hb_offset,
+                                                     InjView inj)
+{
+    constexpr int SPW = 32 / N;  // sites per warp; lanes 32 - 32 % N .. 31 shadow the last site
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / N;
+    const bool used = grp < SPW;
+    const int slot = used ? grp : SPW - 1;
+    const int r = used ? lane - grp * N : lane % N;
+    const int lead = slot * N;  // the lane holding row 0 of this site
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int first = (b - __ldg(bv.begin + l)) * ((int)(blockDim.x >> 5) * SPW) + (int)(threadIdx.x >> 5) * SPW;
+    if (first >= g.halfV) return;  // the whole warp is past the end
+    const int id0 = first + slot;
+    const bool valid = used && id0 < g.halfV;
+    const int id = id0 < g.halfV ? id0 : g.halfV - 1;  // past the end: compute a copy, store nothing
+    typedef LinkIO<N, R, LAYOUT> IO;
+    const cx<R>* base = reinterpret_cast<const cx<R>*>(L.links);
+    const uint32_t V = (uint32_t)g.V, stride = 4u * V;
+
+    int x[4];
+    eo_coords(g, id, parity, x);
+    const int H = g.halfV;
+    const int sx = id + parity * H;
+    const int st[4] = {1, g.X[0], g.X[0] * g.X[1], g.X[0] * g.X[1] * g.X[2]};
+    const int lex = x[0] + st[1] * x[1] + st[2] * x[2] + st[3] * x[3];
+    const int xm = mu == 0 ? x[0] : (mu == 1 ? x[1] : (mu == 2 ? x[2] : x[3]));
+    const int Xm = mu == 0 ? g.X[0] : (mu == 1 ? g.X[1] : (mu == 2 ? g.X[2] : g.X[3]));
+    const int Sm = mu == 0 ? st[0] : (mu == 1 ? st[1] : (mu == 2 ? st[2] : st[3]));
+    const int other = (1 - parity) * H;
+    const int sxpmu = (lex_step(lex, xm, Xm, Sm, 1) >> 1) + other;
+
+    cx<R> Sr[N];  // row r of the staple sum
+#pragma unroll
+    for (int j = 0; j < N; ++j) Sr[j] = mkc<R>(0, 0);
+#pragma unroll
+    for (int nu = 0; nu < 4; ++nu) {
+        if (nu == mu) continue;
+        const int lup = lex_step(lex, x[nu], g.X[nu], st[nu], 1);
+        const int ldn = lex_step(lex, x[nu], g.X[nu], st[nu], -1);
+        const int syp = (lup >> 1) + other;
+        const int sy = (ldn >> 1) + other;
+        const int sz = (lex_step(ldn, xm, Xm, Sm, 1) >> 1) + parity * H;
+        Mat<N, R> A, B;
+        cx<R> a[N], c[N];
+        if constexpr (N == 3 && LAYOUT == L_SOA12) {
+            // rows 0, 1 of the two-link product by lanes 0, 1 (lane 2 repeats
+            // row 0), row 2 rebuilt from them in every lane
+            cx<R> c0[3], c1[3], c2[3];
+            IO::template load_rows<true>(base, sx + nu * V, stride, A);
+            IO::template load<true>(base, syp + mu * V, stride, B);
+            mrow<3, R, 2>(A, r, a);
+            rmul<3, R>(a, B, c);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                c0[j] = shfl_cx(c[j], lead);
+                c1[j] = shfl_cx(c[j], lead + 1);
+            }
+            rebuild12_row<R>(c0, c1, c2);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) c[j] = r == 0 ? c0[j] : (r == 1 ? c1[j] : c2[j]);
+            IO::template load<true>(base, sxpmu + nu * V, stride, A);
+            racc_nd<3, R>(c, A, Sr);
+            // down: U_nu(x-nu)^dagger [U_mu(x-nu) U_nu(x-nu+mu)], the product
+            // needed whole
+            IO::template load_rows<true>(base, sy + mu * V, stride, A);
+            IO::template load<true>(base, sz + nu * V, stride, B);
+            mrow<3, R, 2>(A, r, a);
+            rmul<3, R>(a, B, c);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                c0[j] = shfl_cx(c[j], lead);
+                c1[j] = shfl_cx(c[j], lead + 1);
+            }
+            rebuild12_row<R>(c0, c1, c2);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                B.e[0][j] = c0[j];
+                B.e[1][j] = c1[j];
+                B.e[2][j] = c2[j];
+            }
+            IO::template load<true>(base, sy + nu * V, stride, A);
+            mcol<3, R>(A, r, a);
+            racc_dn<3, R>(a, B, Sr);
+        } else {
+            IO::template load<true>(base, sx + nu * V, stride, A);
+            IO::template load<true>(base, syp + mu * V, stride, B);
+            mrow<N, R>(A, r, a);
+            rmul<N, R>(a, B, c);
+            IO::template load<true>(base, sxpmu + nu * V, stride, A);
+            racc_nd<N, R>(c, A, Sr);
+            IO::template load<true>(base, sy + nu * V, stride, A);
+            IO::template load<true>(base, sy + mu * V, stride, B);
+            mcol<N, R>(A, r, a);
+            rmul_dn<N, R>(a, B, c);
+            IO::template load<true>(base, sz + nu * V, stride, A);
+            racc<N, R>(c, A, Sr);
+        }
+    }
+
+    Mat<N, R> S;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) S.e[i][j] = shfl_cx(Sr[j], lead + i);
+
+    cx<R>* wbase = reinterpret_cast<cx<R>*>(L.links);
+    const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
+    Mat<N, R> U;
+    IO::template load<false>(wbase, own, stride, U);
+    if constexpr (MODE == MODE_OR) {
+        overrelax_update<N, R>(U, S);
+    } else {
+        const R bon = (R)L.beta_over_n;
+        if constexpr (MODE == MODE_HB) {
+            PhiloxStream<R> st;
+            st.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
+            heatbath_update<N, R>(U, S, bon, st);
+        } else {
+            InjectedStream<R> st;
+            st.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
+            st.left = inj.stride;
+            st.err = inj.err;
+            heatbath_update<N, R>(U, S, bon, st);
+        }
+    }
+    if (valid && r == 0) IO::store(wbase, own, stride, U);
+}
+
 // ---------------------------------------------------------------------------
 // Link-wise kernels: work index w over 4V links, w = site * 4 + mu with
 // `site` in the lattice's storage order.
@@ -669,6 +818,19 @@ cudaError_t Ops<N>::update(int fp64, int layout, int mode, const BatchView& bv, 
     if (mode == MODE_OR) k_update<N, R_, L_, MODE_OR><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
     else if (mode == MODE_HB) k_update<N, R_, L_, MODE_HB><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
     else k_update<N, R_, L_, MODE_HB_INJECTED><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::update_rows(int fp64, int layout, int mode, const BatchView& bv, int block, int parity, int mu,
+                                unsigned hb_offset, const InjView& inj, cudaStream_t s)
+{
+#define CALL(R_, L_)                                                                                   \
+    if (mode == MODE_OR) k_update_rows<N, R_, L_, MODE_OR><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
+    else if (mode == MODE_HB) k_update_rows<N, R_, L_, MODE_HB><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
+    else k_update_rows<N, R_, L_, MODE_HB_INJECTED><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
     return cudaGetLastError();

@@ -155,6 +155,97 @@ template <class R> SUN_HD void mmul_rows01(const Mat<3, R>& A, const Mat<3, R>& 
             C.e[i][j] = s;
         }
 }
+// -- one row of the products above, for kernels that spread a matrix over N
+// lanes (lane i owns row i).  Element (i, j) is formed by exactly the same
+// operations, in the same order, as in the whole-matrix routine it names, so
+// the two give the same bits.
+// row r (runtime) of the first ROWS rows of A, by selects (no local memory)
+template <int N, class R, int ROWS = N> SUN_DEV void mrow(const Mat<N, R>& A, int r, cx<R> out[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> v = A.e[0][j];
+#pragma unroll
+        for (int i = 1; i < ROWS; ++i)
+            if (r == i) v = A.e[i][j];
+        out[j] = v;
+    }
+}
+// column c (runtime) of A
+template <int N, class R> SUN_DEV void mcol(const Mat<N, R>& A, int c, cx<R> out[N])
+{
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        cx<R> v = A.e[k][0];
+#pragma unroll
+        for (int i = 1; i < N; ++i)
+            if (c == i) v = A.e[k][i];
+        out[k] = v;
+    }
+}
+// row of A B from the row a of A -- mmul (and mmul_rows01)
+template <int N, class R> SUN_DEV void rmul(const cx<R> a[N], const Mat<N, R>& B, cx<R> c[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> s = a[0] * B.e[0][j];
+#pragma unroll
+        for (int k = 1; k < N; ++k) s = cfma(a[k], B.e[k][j], s);
+        c[j] = s;
+    }
+}
+// row i of A^dagger B from column i of A (a) -- mmul_dn
+template <int N, class R> SUN_DEV void rmul_dn(const cx<R> a[N], const Mat<N, R>& B, cx<R> c[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> s = mkc<R>(0, 0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) s = cfma_cn(a[k], B.e[k][j], s);
+        c[j] = s;
+    }
+}
+// row of S += A B^dagger from the row a of A -- macc_nd
+template <int N, class R> SUN_DEV void racc_nd(const cx<R> a[N], const Mat<N, R>& B, cx<R> s[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> t = s[j];
+#pragma unroll
+        for (int k = 0; k < N; ++k) t = cfma_nc(a[k], B.e[j][k], t);
+        s[j] = t;
+    }
+}
+// row of S += A B from the row a of A -- macc
+template <int N, class R> SUN_DEV void racc(const cx<R> a[N], const Mat<N, R>& B, cx<R> s[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> t = s[j];
+#pragma unroll
+        for (int k = 0; k < N; ++k) t = cfma(a[k], B.e[k][j], t);
+        s[j] = t;
+    }
+}
+// row i of S += A^dagger B from column i of A (a) -- macc_dn
+template <int N, class R> SUN_DEV void racc_dn(const cx<R> a[N], const Mat<N, R>& B, cx<R> s[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> t = s[j];
+#pragma unroll
+        for (int k = 0; k < N; ++k) t = cfma_cn(a[k], B.e[k][j], t);
+        s[j] = t;
+    }
+}
+// row 2 of an SU(3) matrix from rows 0, 1 -- rebuild12
+template <class R> SUN_DEV void rebuild12_row(const cx<R> a[3], const cx<R> b[3], cx<R> c[3])
+{
+    c[0] = cconj(a[1] * b[2] - a[2] * b[1]);
+    c[1] = cconj(a[2] * b[0] - a[0] * b[2]);
+    c[2] = cconj(a[0] * b[1] - a[1] * b[0]);
+}
+
 template <int N, class R> SUN_HD cx<R> mtrace(const Mat<N, R>& A)
 {
     cx<R> t = A.e[0][0];

@@ -46,6 +46,11 @@ template <int N> struct Ops {
     // inside the current sweep)
     static cudaError_t update(int fp64, int layout, int mode, const BatchView& bv, int block,
                               int parity, int mu, unsigned hb_offset, const InjView& inj, cudaStream_t s);
+    // the same phase with the N lanes of a site sharing its staple products
+    // (k_update_rows); block = threads per CTA (a multiple of 32), each warp
+    // covering 32/N sites
+    static cudaError_t update_rows(int fp64, int layout, int mode, const BatchView& bv, int block,
+                                   int parity, int mu, unsigned hb_offset, const InjView& inj, cudaStream_t s);
     static cudaError_t cold(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
     static cudaError_t hot(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
     // FP64 reunitarization; only_due: skip lattices whose sweep counter is not

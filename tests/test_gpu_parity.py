@@ -18,7 +18,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-CASES = [  # (N, dims); T % 4 == 0 takes the two-links-per-thread FP32 kernel
+CASES = [  # (N, dims), cubic and not; N >= 4 and SU(3) FP64 full links run k_update_rows here
     (3, (4, 4, 4, 4)),
     (3, (4, 4, 4, 8)),
     (3, (4, 4, 2, 6)),
