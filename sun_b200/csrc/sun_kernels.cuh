@@ -544,8 +544,12 @@ __global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partial
     const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
     double sp = 0.0, tp = 0.0;
     if (w < g.V) {
+        // threads walk the sites in lexicographic order whatever the storage
+        // order, so the neighbours x + mu, x + nu that a CTA reads are read by
+        // the CTAs beside it at about the same time; walking one even/odd
+        // block after the other fetched every link from DRAM twice
         int x[4];
-        site_coords(L, g, w, x);
+        lex_coords(g, w, x);
 #pragma unroll 1
         for (int mu = 0; mu < 3; ++mu) {
             int xm[4];
@@ -627,7 +631,7 @@ __global__ void __launch_bounds__(64) k_wilson(BatchView bv, int RR, int TT, dou
     for (int i = 0; i < 2 * nres; ++i) acc[i] = 0.0;
     if (w < g.V) {
         int x[4];
-        site_coords(L, g, w, x);
+        lex_coords(g, w, x);  // lexicographic walk, as in k_plaquette
         Mat<N, double> Ls[SUN_WMAX + 1];
 #pragma unroll 1
         for (int mu = 0; mu < 3; ++mu) {
