@@ -137,6 +137,38 @@ def cpu_sample(nthreads=0, reps=1, lattice=None):
     return reps * 5 * (V // 2) / dt, threads, dt
 
 
+def accuracy_report(ctx, g, stream):
+    """Accuracy of the FP32 12-parameter sweep against the FP64 oracle:
+    (1) max |U^dagger U - 1| of the benchmarked lattice after its sweeps
+    (FP64 reunitarization every 10); (2) its plaquette against the oracle's
+    plaquette of the same stored links (both evaluate in FP64); (3) one sweep
+    from a Haar start in FP32 on the GPU and in FP64 by the oracle with the
+    same Philox draws, then both plaquettes: their difference is what FP32
+    storage and arithmetic cost over a sweep."""
+    from oracle import oracle as O
+    from sun_b200 import PlaquetteCUB, Sweep, gauge, unitarity_violation
+    X = list(DIMS)
+    stream.synchronize()
+    out = {"unitarity_max": unitarity_violation(g)}
+    p = PlaquetteCUB(g).Run()
+    po = O.plaquette(g.Get(), X)
+    out["plaquette"] = [p.real, p.imag]
+    out["plaquette_vs_oracle_same_links"] = max(abs(p.real - po[0]), abs(p.imag - po[1]))
+    g1 = gauge(ctx, N=N, dims=DIMS, beta=BETA, atype=1, evenodd=True, prec="f32", seed=SEED + 7,
+               reunit_every=REUNIT)
+    g1.Init(hot=True)
+    U = g1.Get()
+    Sweep(g1, 1, 4, 1)
+    p1 = PlaquetteCUB(g1).Run()
+    g1.Release()
+    O.sweeps(U, X, BETA, 1, 4, 1, mode=O.RNG_PHILOX32, seed=SEED + 7)
+    po1 = O.plaquette(U, X)
+    out["one_sweep_from_haar"] = {"plaquette_f32_gpu": [p1.real, p1.imag], "plaquette_f64_oracle": [po1[0], po1[1]],
+                                  "abs_diff": max(abs(p1.real - po1[0]), abs(p1.imag - po1[1])),
+                                  "draws": "the same Philox stream (24-bit uniforms) on both sides"}
+    return out
+
+
 def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
@@ -300,6 +332,7 @@ def main():
     stream.synchronize()
     t_hb = e0.elapsed_time(e1) / 1e3 / (8 * n_hbp)
     clk = clocks.stop()
+    accuracy = accuracy_report(ctx, g, stream) if rank == 0 and not args.no_cpu else None
 
     # end to end through the C ABI with host buffers.  Serial form: upload the
     # image from pinned memory, one sweep, plaquette to the host, download.
@@ -398,12 +431,19 @@ def main():
                    "serial": {"value": world * 20 * V * k_ser / t_ser, "unit": "link-updates/s",
                               "h2d_bytes_per_step": img_bytes, "d2h_bytes_per_step": img_bytes + 16,
                               "step": "upload image + 1 sweep + plaquette + download image, one stream"}}
+    if accuracy is not None:
+        line["accuracy"] = accuracy
     line.update(extras)
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, threads, dt = cpu_sample()
+        # about 10 s of CPU work: repeat the 1/8-sweep sample on one lattice
+        from oracle import oracle as O
+        U = O.hot(N, list(DIMS), SEED)
+        _, _, dt1 = cpu_sample(lattice=U)
+        reps = max(1, min(60, int(10.0 / max(dt1, 1e-3))))
+        rate, threads, dt = cpu_sample(reps=reps, lattice=U)
         line["cpu_baseline"] = {"value": rate, "unit": "link-updates/s", "cores": threads, "kind": "port",
-                                "sample": f"1/8 sweep (one heatbath + four overrelaxation phases, parity 0 mu 0) "
-                                          f"of the 32^4 lattice, FP64 oracle, {dt:.1f} s"}
+                                "sample": f"{reps} x 1/8 sweep (one heatbath + four overrelaxation phases, parity 0 "
+                                          f"mu 0) of the 32^4 lattice, FP64 oracle, {dt:.1f} s"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.Release()

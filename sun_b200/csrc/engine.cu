@@ -626,7 +626,9 @@ sun_status sun_init(const sun_config* cfg, sun_ctx** out)
                     if (!c1) continue;
                     *c1 = 0;
                     int blk = atoi(c1 + 1);
-                    if (blk >= 32 && blk <= 128 && blk % 32 == 0) c->tuned[line] = blk;
+                    // k_update CTA sizes, or k_update_rows ones as negative numbers
+                    const int t = blk < 0 ? -blk : blk;
+                    if (t >= 32 && t <= 128 && t % 32 == 0) c->tuned[line] = blk;
                 }
                 fclose(f);
             }

@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)
     const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
     Mat<N, R> U;
     IO::template load<false>(wbase, own, stride, U);
+    if constexpr (N == 3 && LAYOUT == L_SOA12) unit_row2<R>(U);
     if constexpr (MODE == MODE_OR) {
         overrelax_update<N, R>(U, S);
     } else {
@@ -312,6 +313,7 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
     const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
     Mat<N, R> U;
     IO::template load<false>(wbase, own, stride, U);
+    if constexpr (N == 3 && LAYOUT == L_SOA12) unit_row2<R>(U);
     if constexpr (MODE == MODE_OR) {
         overrelax_update<N, R>(U, S);
     } else {

@@ -365,6 +365,25 @@ template <class R> SUN_HD void rebuild12(Mat<3, R>& A)
     A.e[2][2] = cconj(A.e[0][0] * A.e[1][1] - A.e[0][1] * A.e[1][0]);
 }
 
+SUN_DEV float rsq(float x) { return rsqrtf(x); }
+SUN_DEV double rsq(double x) { return rsqrt(x); }
+
+// The link a 12-parameter update rewrites: its rebuilt row 2 scaled to unit
+// length.  The update rotates row 2 into the two stored rows.  Unscaled,
+// |row2|^2 - 1 ~ (|row0|^2 - 1) + (|row1|^2 - 1) is fed back into them, and
+// the storage error grows about 4x per sweep: FP32 links measured on B200
+// reach |U^dag U - 1| ~ 0.5 in 9 sweeps and overflow in 13 without
+// reunitarization (FP64: 1e-13 to 3e-5 in 16 sweeps).  The reference's
+// reconstruction (reconstruct_12p_8p.h:17-21) grows the same way.  Scaled,
+// each rotation shrinks the norm and orthogonality errors of the stored rows
+// instead, and the error stays at the rounding level of full links.
+template <class R> SUN_DEV void unit_row2(Mat<3, R>& A)
+{
+    const R s = rsq(cnorm2(A.e[2][0]) + cnorm2(A.e[2][1]) + cnorm2(A.e[2][2]));
+#pragma unroll
+    for (int j = 0; j < 3; ++j) A.e[2][j] = s * A.e[2][j];
+}
+
 // Determinant; N <= 3 by cofactors, larger N by Gaussian elimination with
 // partial pivoting (used only by FP64 reunitarization and the hot start).
 template <int N, class R> SUN_DEV cx<R> mdet(const Mat<N, R>& A)

@@ -92,6 +92,30 @@ def test_cold_start(ctx, case):
     assert abs(OnePolyakovLoop(g).Run() - 1) < 1e-12
 
 
+@pytest.mark.parametrize("prec,lay,bound", [("f32", 1, 1e-5), ("f64", 1, 1e-13), ("f32", 0, 3e-5)])
+def test_unitarity_stays_bounded_without_reunitarization(ctx, prec, lay, bound):
+    """16 sweeps with no reunitarization: the 12-parameter update (the
+    rewritten link's rebuilt row scaled to unit length) keeps |U^dag U - 1|
+    at its rounding level, as full links do, instead of growing ~4x per sweep."""
+    from sun_b200 import Sweep, unitarity_violation
+    g = _make(ctx, 3, (8, 8, 8, 8), prec, lay, beta=6.0, seed=5)
+    g.Init(hot=True)
+    worst = 0.0
+    for _ in range(16):
+        Sweep(g, 1, 4, 1)
+        worst = max(worst, unitarity_violation(g))
+    assert worst < bound, worst
+
+
+def test_lattice_beyond_32bit_indexing_refused(ctx):
+    """96^4 SU(3) full links: 4V x 9 elements pass 2^31, so the lattice is
+    refused before any allocation."""
+    from sun_b200 import SunError
+    with pytest.raises(SunError) as e:
+        _make(ctx, 3, (96, 96, 96, 96), "f64", 0)
+    assert e.value.status == 7
+
+
 def test_soa8_cold_start_refused(ctx):
     from sun_b200 import SunError
     g = _make(ctx, 3, (4, 4, 4, 4), "f32", 2)
