@@ -389,6 +389,12 @@ def main():
         extras["smearing"] = smear_bench(ctx, L, sp, stream)
         if rank == 0:
             extras["serving"] = serving_bench(ctx)
+            # the same job mix at a rate the GPU keeps up with: latency is then
+            # service time (jobs overlapping on the device), not queueing
+            light = serving_bench(ctx, rate=2.0, window=6.0)
+            extras["serving"]["light_load"] = {k: light[k] for k in ("jobs", "completed", "arrival_rate_per_s",
+                                                                      "window_s", "p50_latency_s", "p99_latency_s",
+                                                                      "link_updates_per_s", "wall_s")}
 
     line = {
         "metric": "link-updates/s",

@@ -372,6 +372,32 @@ def test_batch_identical_alone_and_mixed(ctx):
         assert bp[i, 0] == p.real and bp[i, 1] == p.imag
 
 
+def test_solo_sweep_graph_matches_direct_launches(ctx):
+    """sun_sweep replays one captured sweep; a batch without a graph
+    launches every kernel directly.  Both give the same bits, also after the
+    RNG state is reset between calls (which re-captures the solo graph) and
+    with the passes per sweep changing."""
+    from sun_b200 import Batch, Sweep
+    for prec, lay in (("f64", 0), ("f32", 1)):
+        a = _make(ctx, 3, (4, 4, 4, 8), prec, lay, beta=5.9, seed=71, reunit_every=2)
+        b = _make(ctx, 3, (4, 4, 4, 8), prec, lay, beta=5.9, seed=71, reunit_every=2)
+        a.Init(hot=True)
+        b.Init(hot=True)
+        batch = Batch(ctx)
+        batch.add(b)
+        Sweep(a, 1, 4, 3)
+        batch.sweep(1, 4, 3)
+        for g in (a, b):
+            g.set_rng_state(99, 5, 7)
+        Sweep(a, 1, 4, 2)
+        Sweep(a, 2, 1, 1)
+        batch.sweep(1, 4, 2)
+        batch.sweep(2, 1, 1)
+        assert np.array_equal(a.get_image(), b.get_image())
+        assert a.rng_state() == b.rng_state()
+        batch.close()
+
+
 def test_server_result_independent_of_mix(ctx):
     from sun_b200 import Server, make_job
     job = make_job(N=3, dims=(4, 4, 4, 8), beta=5.8, sweeps=6, seed=11, observables=7, R=2, T=2)
