@@ -138,6 +138,9 @@ struct sun_ctx {
     // thread per half-site.
     int upd_kernel = 0;
     int blk_rows = 128;
+    // consecutive update phases launched as programmatic dependents
+    // (SUN_B200_PDL=0 turns it off)
+    int pdl = 1;
     long long rows_max_halfv = 16384;
     // autotuner (tuneLaunch, src/tune.cpp:304): CTA size of the update kernel
     // per (kernel class, total half-volume), timed once, cached in a CSV file
@@ -261,11 +264,13 @@ int upd_sites_per_cta(int N, int cfg) { return cfg > 0 ? cfg : (-cfg / 32) * (32
 
 BatchView upd_view(Group& g, int cfg, cudaStream_t s) { return g.view(WORK_HALF, upd_sites_per_cta(g.N, cfg), s); }
 
+// pdl: launch as a programmatic dependent of the previous launch on s, which
+// must be the preceding update phase of the same lattices
 void launch_update(Group& g, int mode, int cfg, const BatchView& v, int par, int mu, unsigned hb_offset,
-                   const InjView& inj, cudaStream_t s)
+                   const InjView& inj, cudaStream_t s, int pdl = 0)
 {
-    if (cfg > 0) OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, cfg, par, mu, hb_offset, inj, s);
-    else OPS_CALL(g.N, update_rows, g.fp64, g.layout, mode, v, -cfg, par, mu, hb_offset, inj, s);
+    if (cfg > 0) OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, cfg, par, mu, hb_offset, inj, pdl, s);
+    else OPS_CALL(g.N, update_rows, g.fp64, g.layout, mode, v, -cfg, par, mu, hb_offset, inj, pdl, s);
 }
 
 // Update launch shape for this group and mode.  Without tuning: by the size
@@ -347,20 +352,25 @@ void group_sweep(sun_ctx* c, Group& g, int n_hb, int n_or, bool count_sweep, boo
     if (g.lats.empty()) return;
     InjView none{nullptr, 0, nullptr};
     // a shape's table is made only for a mode that runs: inside a graph
-    // capture only the tables prepared before it exist
+    // capture only the tables prepared before it exist.  Every phase after
+    // the first is launched as a programmatic dependent of the one before
+    // (its launch overlaps the previous phase's drain).
+    int pdl = 0;
     if (n_hb > 0) {
         const int bhb = update_block(c, g, MODE_HB, s);
         BatchView vhb = upd_view(g, bhb, s);
         for (int h = 0; h < n_hb; ++h)
             for (int par = 0; par < 2; ++par)
-                for (int mu = 0; mu < 4; ++mu) launch_update(g, MODE_HB, bhb, vhb, par, mu, (unsigned)h, none, s);
+                for (int mu = 0; mu < 4; ++mu, pdl = c->pdl)
+                    launch_update(g, MODE_HB, bhb, vhb, par, mu, (unsigned)h, none, s, pdl);
     }
     if (n_or > 0) {
         const int bor = update_block(c, g, MODE_OR, s);
         BatchView vor = upd_view(g, bor, s);
         for (int o = 0; o < n_or; ++o)
             for (int par = 0; par < 2; ++par)
-                for (int mu = 0; mu < 4; ++mu) launch_update(g, MODE_OR, bor, vor, par, mu, 0u, none, s);
+                for (int mu = 0; mu < 4; ++mu, pdl = c->pdl)
+                    launch_update(g, MODE_OR, bor, vor, par, mu, 0u, none, s, pdl);
     }
     if (n_hb > 0 || count_sweep)
         ck(launch_end_sweep(reinterpret_cast<const LatDev*>(g.d_lats.p), (int)g.lats.size(), (unsigned)n_hb,
@@ -672,6 +682,7 @@ sun_status sun_init(const sun_config* cfg, sun_ctx** out)
             else if (!strcmp(k, "rows")) c->upd_kernel = 2;
         }
         if (const char* t = getenv("SUN_B200_ROWS_MAX_HALFV")) c->rows_max_halfv = atoll(t);
+        if (const char* t = getenv("SUN_B200_PDL")) c->pdl = atoi(t) ? 1 : 0;
         *out = c.release();
     });
 }

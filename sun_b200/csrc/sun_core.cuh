@@ -331,11 +331,17 @@ template <class R> struct Vec2;
 template <> struct Vec2<float> { typedef float2 T; };
 template <> struct Vec2<double> { typedef double2 T; };
 
-template <class R, bool NC> SUN_DEV cx<R> ld_elem(const cx<R>* p)
+// Load paths of a link element: LD_CA plain (coherent, L1-cached), LD_NC the
+// read-only path (data constant for the kernel's lifetime), LD_CG L2 only.
+// The update kernels, which overlap the previous phase's launch, read
+// through L2 only: lines an SM's L1 held across the overlap were seen stale.
+enum { LD_CA = 0, LD_NC = 1, LD_CG = 2 };
+template <class R, int P> SUN_DEV cx<R> ld_elem(const cx<R>* p)
 {
     typedef typename Vec2<R>::T V2;
     V2 v;
-    if (NC) v = __ldg(reinterpret_cast<const V2*>(p));
+    if (P == LD_NC) v = __ldg(reinterpret_cast<const V2*>(p));
+    else if (P == LD_CG) v = __ldcg(reinterpret_cast<const V2*>(p));
     else v = *reinterpret_cast<const V2*>(p);
     return mkc<R>(v.x, v.y);
 }
@@ -376,13 +382,13 @@ template <class R> SUN_DEV void rebuild8(Mat<3, R>& A, R th0, R th2)
 template <int N, class R, int LAYOUT> struct LinkIO {
     static constexpr int NE = LayoutInfo<N, LAYOUT>::elems;
     // SOA12: the two stored rows only, row 2 left unset
-    template <bool NC> static SUN_DEV void load_rows(const cx<R>* base, uint32_t idx, uint32_t stride, Mat<N, R>& A)
+    template <int NC> static SUN_DEV void load_rows(const cx<R>* base, uint32_t idx, uint32_t stride, Mat<N, R>& A)
     {
         static_assert(LAYOUT == L_SOA12, "stored rows exist for SOA12 only");
 #pragma unroll
         for (int e = 0; e < 6; ++e) A.e[e / 3][e % 3] = ld_elem<R, NC>(base + idx + e * stride);
     }
-    template <bool NC> static SUN_DEV void load(const cx<R>* base, uint32_t idx, uint32_t stride, Mat<N, R>& A)
+    template <int NC> static SUN_DEV void load(const cx<R>* base, uint32_t idx, uint32_t stride, Mat<N, R>& A)
     {
         if constexpr (LAYOUT == L_SOA) {
 #pragma unroll

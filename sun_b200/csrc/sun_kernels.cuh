@@ -84,11 +84,11 @@ template <class R, int MODE> struct UpdateOccupancy<3, R, MODE> {
 // kernel_PHeatBath_evenodd (src/monte/monte.cu:44-88) and
 // kernel_overrelaxation_evenodd (src/monte/ovr.cu:41-80).  One thread per
 // half-lattice site; the staple sum keeps the reference's order (nu ascending,
-// "up" then "down"); neighbour links are read through the read-only path
-// (they are never written in this phase), the own link through plain loads.
+// "up" then "down"); all links are read through L2 only (LD_CG: the launch
+// overlaps the previous phase's, see the pdl note below).
 template <int N, class R, int LAYOUT, int MODE>
 __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
-                                                InjView inj)
+                                                InjView inj, int pdl)
 {
     const int b = blockIdx.x;
     const int l = find_lat(bv, b);
@@ -114,11 +114,23 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)
     const int other = (1 - parity) * H;
     const int sxpmu = (lex_step(lex, xm, Xm, Sm, 1) >> 1) + other;
 
+    // launched as a programmatic dependent of the previous phase (pdl): that
+    // phase wrote the links of direction dep = mu - 1 (mod 4), which only
+    // the staples of nu = dep read.  The staples before it in the reference's
+    // order are summed while the previous launch drains; griddepcontrol.wait
+    // then waits for it to complete, and only after that the next phase may
+    // launch (so a launch never runs beside the one two back).
+    const int dep = pdl ? ((mu + 3) & 3) : -1;
+    if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     Mat<N, R> S;
     mzero(S);
 #pragma unroll
     for (int nu = 0; nu < 4; ++nu) {
         if (nu == mu) continue;
+        if (nu == dep) {
+            asm volatile("griddepcontrol.wait;" ::: "memory");
+            asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+        }
         const int lup = lex_step(lex, x[nu], g.X[nu], st[nu], 1);
         const int ldn = lex_step(lex, x[nu], g.X[nu], st[nu], -1);
         const int syp = (lup >> 1) + other;                               // x + nu
@@ -130,31 +142,31 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)
             // only its rows 0, 1 are multiplied out (from the stored rows of
             // the left factor, which is not rebuilt) and row 2 is rebuilt as
             // conj(row0 x row1) -- 36 fewer real FMAs per staple
-            IO::template load_rows<true>(base, sx + nu * V, stride, A);
-            IO::template load<true>(base, syp + mu * V, stride, B);
+            IO::template load_rows<LD_CG>(base, sx + nu * V, stride, A);
+            IO::template load<LD_CG>(base, syp + mu * V, stride, B);
             mmul_rows01(A, B, C);
             rebuild12(C);
-            IO::template load<true>(base, sxpmu + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sxpmu + nu * V, stride, A);
             macc_nd(C, A, S);
             // down: U_nu(x-nu)^dagger [U_mu(x-nu) U_nu(x-nu+mu)]
-            IO::template load_rows<true>(base, sy + mu * V, stride, A);
-            IO::template load<true>(base, sz + nu * V, stride, B);
+            IO::template load_rows<LD_CG>(base, sy + mu * V, stride, A);
+            IO::template load<LD_CG>(base, sz + nu * V, stride, B);
             mmul_rows01(A, B, C);
             rebuild12(C);
-            IO::template load<true>(base, sy + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sy + nu * V, stride, A);
             macc_dn(A, C, S);
         } else {
             // up: U_nu(x) U_mu(x+nu) U_nu(x+mu)^dagger
-            IO::template load<true>(base, sx + nu * V, stride, A);
-            IO::template load<true>(base, syp + mu * V, stride, B);
+            IO::template load<LD_CG>(base, sx + nu * V, stride, A);
+            IO::template load<LD_CG>(base, syp + mu * V, stride, B);
             mmul(A, B, C);
-            IO::template load<true>(base, sxpmu + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sxpmu + nu * V, stride, A);
             macc_nd(C, A, S);
             // down: U_nu(x-nu)^dagger U_mu(x-nu) U_nu(x-nu+mu)
-            IO::template load<true>(base, sy + nu * V, stride, A);
-            IO::template load<true>(base, sy + mu * V, stride, B);
+            IO::template load<LD_CG>(base, sy + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sy + mu * V, stride, B);
             mmul_dn(A, B, C);
-            IO::template load<true>(base, sz + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sz + nu * V, stride, A);
             macc(C, A, S);
         }
     }
@@ -162,7 +174,7 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)
     cx<R>* wbase = reinterpret_cast<cx<R>*>(L.links);
     const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
     Mat<N, R> U;
-    IO::template load<false>(wbase, own, stride, U);
+    IO::template load<LD_CG>(wbase, own, stride, U);
     if constexpr (N == 3 && LAYOUT == L_SOA12) unit_row2<R>(U);
     if constexpr (MODE == MODE_OR) {
         overrelax_update<N, R>(U, S);
@@ -201,7 +213,7 @@ template <class R> SUN_DEV cx<R> shfl_cx(cx<R> v, int src)
 // may run any lattice.
 template <int N, class R, int LAYOUT, int MODE>
 __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, int mu, unsigned hb_offset,
-                                                     InjView inj)
+                                                     InjView inj, int pdl)
 {
     constexpr int SPW = 32 / N;  // sites per warp; lanes 32 - 32 % N .. 31 shadow the last site
     const int lane = threadIdx.x & 31;
@@ -235,12 +247,18 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
     const int other = (1 - parity) * H;
     const int sxpmu = (lex_step(lex, xm, Xm, Sm, 1) >> 1) + other;
 
+    const int dep = pdl ? ((mu + 3) & 3) : -1;  // as in k_update
+    if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     cx<R> Sr[N];  // row r of the staple sum
 #pragma unroll
     for (int j = 0; j < N; ++j) Sr[j] = mkc<R>(0, 0);
 #pragma unroll
     for (int nu = 0; nu < 4; ++nu) {
         if (nu == mu) continue;
+        if (nu == dep) {
+            asm volatile("griddepcontrol.wait;" ::: "memory");
+            asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+        }
         const int lup = lex_step(lex, x[nu], g.X[nu], st[nu], 1);
         const int ldn = lex_step(lex, x[nu], g.X[nu], st[nu], -1);
         const int syp = (lup >> 1) + other;
@@ -252,8 +270,8 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
             // rows 0, 1 of the two-link product by lanes 0, 1 (lane 2 repeats
             // row 0), row 2 rebuilt from them in every lane
             cx<R> c0[3], c1[3], c2[3];
-            IO::template load_rows<true>(base, sx + nu * V, stride, A);
-            IO::template load<true>(base, syp + mu * V, stride, B);
+            IO::template load_rows<LD_CG>(base, sx + nu * V, stride, A);
+            IO::template load<LD_CG>(base, syp + mu * V, stride, B);
             mrow<3, R, 2>(A, r, a);
             rmul<3, R>(a, B, c);
 #pragma unroll
@@ -264,12 +282,12 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
             rebuild12_row<R>(c0, c1, c2);
 #pragma unroll
             for (int j = 0; j < 3; ++j) c[j] = r == 0 ? c0[j] : (r == 1 ? c1[j] : c2[j]);
-            IO::template load<true>(base, sxpmu + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sxpmu + nu * V, stride, A);
             racc_nd<3, R>(c, A, Sr);
             // down: U_nu(x-nu)^dagger [U_mu(x-nu) U_nu(x-nu+mu)], the product
             // needed whole
-            IO::template load_rows<true>(base, sy + mu * V, stride, A);
-            IO::template load<true>(base, sz + nu * V, stride, B);
+            IO::template load_rows<LD_CG>(base, sy + mu * V, stride, A);
+            IO::template load<LD_CG>(base, sz + nu * V, stride, B);
             mrow<3, R, 2>(A, r, a);
             rmul<3, R>(a, B, c);
 #pragma unroll
@@ -284,21 +302,21 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
                 B.e[1][j] = c1[j];
                 B.e[2][j] = c2[j];
             }
-            IO::template load<true>(base, sy + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sy + nu * V, stride, A);
             mcol<3, R>(A, r, a);
             racc_dn<3, R>(a, B, Sr);
         } else {
-            IO::template load<true>(base, sx + nu * V, stride, A);
-            IO::template load<true>(base, syp + mu * V, stride, B);
+            IO::template load<LD_CG>(base, sx + nu * V, stride, A);
+            IO::template load<LD_CG>(base, syp + mu * V, stride, B);
             mrow<N, R>(A, r, a);
             rmul<N, R>(a, B, c);
-            IO::template load<true>(base, sxpmu + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sxpmu + nu * V, stride, A);
             racc_nd<N, R>(c, A, Sr);
-            IO::template load<true>(base, sy + nu * V, stride, A);
-            IO::template load<true>(base, sy + mu * V, stride, B);
+            IO::template load<LD_CG>(base, sy + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sy + mu * V, stride, B);
             mcol<N, R>(A, r, a);
             rmul_dn<N, R>(a, B, c);
-            IO::template load<true>(base, sz + nu * V, stride, A);
+            IO::template load<LD_CG>(base, sz + nu * V, stride, A);
             racc<N, R>(c, A, Sr);
         }
     }
@@ -312,7 +330,7 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
     cx<R>* wbase = reinterpret_cast<cx<R>*>(L.links);
     const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
     Mat<N, R> U;
-    IO::template load<false>(wbase, own, stride, U);
+    IO::template load<LD_CG>(wbase, own, stride, U);
     if constexpr (N == 3 && LAYOUT == L_SOA12) unit_row2<R>(U);
     if constexpr (MODE == MODE_OR) {
         overrelax_update<N, R>(U, S);
@@ -816,30 +834,51 @@ __global__ void __launch_bounds__(256) k_unpack(BatchView bv, double2* canon)
         }                                                                           \
     } while (0)
 
+// One update launch; pdl: as a programmatic dependent of the launch before
+// it on the stream (which must be the previous update phase).
+template <class K>
+cudaError_t launch_phase(K kernel, const BatchView& bv, int block, int parity, int mu, unsigned hb_offset,
+                         const InjView& inj, int pdl, cudaStream_t s)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)bv.nblocks);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, bv, parity, mu, hb_offset, inj, pdl);
+}
+
 template <int N>
 cudaError_t Ops<N>::update(int fp64, int layout, int mode, const BatchView& bv, int block, int parity, int mu,
-                           unsigned hb_offset, const InjView& inj, cudaStream_t s)
+                           unsigned hb_offset, const InjView& inj, int pdl, cudaStream_t s)
 {
-#define CALL(R_, L_)                                                                                   \
-    if (mode == MODE_OR) k_update<N, R_, L_, MODE_OR><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
-    else if (mode == MODE_HB) k_update<N, R_, L_, MODE_HB><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
-    else k_update<N, R_, L_, MODE_HB_INJECTED><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj)
+    cudaError_t e = cudaSuccess;
+#define CALL(R_, L_)                                                                                          \
+    if (mode == MODE_OR) e = launch_phase(k_update<N, R_, L_, MODE_OR>, bv, block, parity, mu, hb_offset, inj, pdl, s); \
+    else if (mode == MODE_HB) e = launch_phase(k_update<N, R_, L_, MODE_HB>, bv, block, parity, mu, hb_offset, inj, pdl, s); \
+    else e = launch_phase(k_update<N, R_, L_, MODE_HB_INJECTED>, bv, block, parity, mu, hb_offset, inj, pdl, s)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int N>
 cudaError_t Ops<N>::update_rows(int fp64, int layout, int mode, const BatchView& bv, int block, int parity, int mu,
-                                unsigned hb_offset, const InjView& inj, cudaStream_t s)
+                                unsigned hb_offset, const InjView& inj, int pdl, cudaStream_t s)
 {
-#define CALL(R_, L_)                                                                                   \
-    if (mode == MODE_OR) k_update_rows<N, R_, L_, MODE_OR><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
-    else if (mode == MODE_HB) k_update_rows<N, R_, L_, MODE_HB><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj); \
-    else k_update_rows<N, R_, L_, MODE_HB_INJECTED><<<bv.nblocks, block, 0, s>>>(bv, parity, mu, hb_offset, inj)
+    cudaError_t e = cudaSuccess;
+#define CALL(R_, L_)                                                                                               \
+    if (mode == MODE_OR) e = launch_phase(k_update_rows<N, R_, L_, MODE_OR>, bv, block, parity, mu, hb_offset, inj, pdl, s); \
+    else if (mode == MODE_HB) e = launch_phase(k_update_rows<N, R_, L_, MODE_HB>, bv, block, parity, mu, hb_offset, inj, pdl, s); \
+    else e = launch_phase(k_update_rows<N, R_, L_, MODE_HB_INJECTED>, bv, block, parity, mu, hb_offset, inj, pdl, s)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 template <int N> cudaError_t Ops<N>::cold(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s)

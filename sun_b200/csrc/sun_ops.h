@@ -44,13 +44,18 @@ template <int N> struct Ops {
     // one checkerboard phase (parity, mu) of heatbath or overrelaxation;
     // hb_offset is added to the lattice's pass counter (heatbath pass index
     // inside the current sweep)
+    // pdl: launch as a programmatic dependent of the previous launch on the
+    // stream, which must be the update phase (parity, mu - 1) or, for mu = 0,
+    // (1 - parity, 3); the kernel then waits for it only before the staples
+    // of that phase's direction
     static cudaError_t update(int fp64, int layout, int mode, const BatchView& bv, int block,
-                              int parity, int mu, unsigned hb_offset, const InjView& inj, cudaStream_t s);
+                              int parity, int mu, unsigned hb_offset, const InjView& inj, int pdl, cudaStream_t s);
     // the same phase with the N lanes of a site sharing its staple products
     // (k_update_rows); block = threads per CTA (a multiple of 32), each warp
     // covering 32/N sites
     static cudaError_t update_rows(int fp64, int layout, int mode, const BatchView& bv, int block,
-                                   int parity, int mu, unsigned hb_offset, const InjView& inj, cudaStream_t s);
+                                   int parity, int mu, unsigned hb_offset, const InjView& inj, int pdl,
+                                   cudaStream_t s);
     static cudaError_t cold(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
     static cudaError_t hot(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
     // FP64 reunitarization; only_due: skip lattices whose sweep counter is not
