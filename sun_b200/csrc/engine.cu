@@ -194,6 +194,8 @@ struct Group {
     };
     std::map<std::pair<int, int>, Begin> begins;
     DevBuf partials, out;
+    DevBuf counters;     // per-lattice CTA counters of the fused finalize (kept at zero)
+    size_t counters_n = 0;
     PinnedBuf h_out;
     bool dirty = true;
     std::vector<unsigned> versions;
@@ -414,11 +416,31 @@ template <class F> double* group_reduce(Group& g, int kind, int block, int nvals
     return reinterpret_cast<double*>(g.h_out.p);
 }
 
+// The same for kernels that finalize in their last CTA per lattice and write
+// the result straight into the pinned host buffer: one launch and a
+// synchronisation, no finalize launch and no copy.
+template <class F> double* group_reduce_fused(Group& g, int kind, int block, int nvals, cudaStream_t s, F launch)
+{
+    BatchView v = g.view(kind, block, s);
+    g.partials.ensure(sizeof(double) * 2 * (size_t)nvals * std::max(1, v.nblocks));
+    g.h_out.ensure(sizeof(double) * (size_t)nvals * g.lats.size());
+    if (g.counters_n < g.lats.size()) {
+        g.counters.ensure(sizeof(unsigned) * g.lats.size());
+        ck(cudaMemsetAsync(g.counters.p, 0, sizeof(unsigned) * g.lats.size(), s), "counters");
+        g.counters_n = g.lats.size();
+    }
+    launch(v, reinterpret_cast<double*>(g.partials.p), reinterpret_cast<double*>(g.h_out.p),
+           reinterpret_cast<unsigned*>(g.counters.p));
+    ck(cudaStreamSynchronize(s), "measurement");
+    return reinterpret_cast<double*>(g.h_out.p);
+}
+
 void group_plaquette(sun_ctx* c, Group& g, double* out, cudaStream_t s)
 {
-    double* r = group_reduce(g, WORK_SITES, c->blk_sites, 2, false, s, [&](const BatchView& v, double* part) {
-        OPS_CALL(g.N, plaquette, g.fp64, g.layout, v, c->blk_sites, part, s);
-    });
+    double* r = group_reduce_fused(g, WORK_SITES, c->blk_sites, 2, s,
+                                   [&](const BatchView& v, double* part, double* out, unsigned* cnt) {
+                                       OPS_CALL(g.N, plaquette, g.fp64, g.layout, v, c->blk_sites, part, out, cnt, s);
+                                   });
     for (size_t i = 0; i < g.lats.size(); ++i) {
         const LatDev& L = g.lats[i]->desc;
         double norm = 3.0 * g.N * (double)L.V;
@@ -429,9 +451,10 @@ void group_plaquette(sun_ctx* c, Group& g, double* out, cudaStream_t s)
 
 void group_polyakov(sun_ctx* c, Group& g, double* out, cudaStream_t s)
 {
-    double* r = group_reduce(g, WORK_SPATIAL, c->blk_sites, 2, false, s, [&](const BatchView& v, double* part) {
-        OPS_CALL(g.N, polyakov, g.fp64, g.layout, v, c->blk_sites, part, s);
-    });
+    double* r = group_reduce_fused(g, WORK_SPATIAL, c->blk_sites, 2, s,
+                                   [&](const BatchView& v, double* part, double* out, unsigned* cnt) {
+                                       OPS_CALL(g.N, polyakov, g.fp64, g.layout, v, c->blk_sites, part, out, cnt, s);
+                                   });
     for (size_t i = 0; i < g.lats.size(); ++i) {
         const LatDev& L = g.lats[i]->desc;
         double norm = (double)g.N * L.X[0] * L.X[1] * L.X[2];

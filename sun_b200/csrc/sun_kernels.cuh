@@ -508,6 +508,41 @@ SUN_DEV void block_sum(double v, double* out, DD* sh)
     }
     __syncthreads();
 }
+// Finalize of lattice l's CTA partials, run by the last of its CTAs to
+// finish (each CTA fences its partials, then counts itself in): the same
+// lane-strided compensated sums and shuffle tree as k_finalize_sum, so the
+// result is the same whichever CTA runs it.  The result goes straight to
+// out (host-mapped memory allowed); the counter is left at zero.
+SUN_DEV void finalize_if_last(const BatchView& bv, int l, const double* partials, int nvals, double* out,
+                              unsigned* counters)
+{
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned n = (unsigned)(__ldg(bv.begin + l + 1) - __ldg(bv.begin + l));
+        last = atomicAdd(counters + l, 1u) == n - 1u;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x >= 32) return;
+    __threadfence();
+    const int lane = threadIdx.x;
+    const int b0 = __ldg(bv.begin + l), b1 = __ldg(bv.begin + l + 1);
+    for (int v = 0; v < nvals; ++v) {
+        DD d;
+        d.s = 0.0; d.c = 0.0;
+        for (int b = b0 + lane; b < b1; b += 32) {
+            DD t;
+            t.s = __ldcg(partials + ((size_t)b * nvals + v) * 2);
+            t.c = __ldcg(partials + ((size_t)b * nvals + v) * 2 + 1);
+            d = dd_add(d, t);
+        }
+        d = dd_warp(d);
+        if (lane == 0) out[(size_t)l * nvals + v] = d.s + d.c;
+    }
+    if (lane == 0) counters[l] = 0u;
+}
+
 SUN_DEV void block_max(double v, double* out, double* sh)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -554,7 +589,7 @@ SUN_DEV void load_d(const LatDev& L, const Geom& g, const int x[4], int mu, Mat<
 // Re tr[U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag], nu == 3 temporal.
 // Links are widened to FP64 before the products.
 template <int N, class R, int LAYOUT>
-__global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partials)
+__global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partials, double* out, unsigned* counters)
 {
     __shared__ DD sh[32];
     const int b = blockIdx.x;
@@ -592,13 +627,14 @@ __global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partial
     }
     block_sum(sp, partials + (size_t)b * 4, sh);
     block_sum(tp, partials + (size_t)b * 4 + 2, sh);
+    if (out) finalize_if_last(bv, l, partials, 2, out, counters);
 }
 
 // Polyakov loop -- kernel_calc_polyakovloop_evenodd
 // (src/meas/polyakovloop.cu:54-96): one thread per spatial site,
 // L = U_3(x,0) U_3(x,1) ... U_3(x,T-1), trace summed.
 template <int N, class R, int LAYOUT>
-__global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials)
+__global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials, double* out, unsigned* counters)
 {
     __shared__ DD sh[32];
     const int b = blockIdx.x;
@@ -629,6 +665,7 @@ __global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials
     }
     block_sum(re, partials + (size_t)b * 4, sh);
     block_sum(im, partials + (size_t)b * 4 + 2, sh);
+    if (out) finalize_if_last(bv, l, partials, 2, out, counters);
 }
 
 // Planar Wilson loops W(r,t), r <= R, t <= T, averaged over the 3 spatial
@@ -908,9 +945,9 @@ cudaError_t Ops<N>::reunit(int fp64, int layout, const BatchView& bv, int block,
 
 template <int N>
 cudaError_t Ops<N>::plaquette(int fp64, int layout, const BatchView& bv, int block, double* partials,
-                              cudaStream_t s)
+                              double* out, unsigned* counters, cudaStream_t s)
 {
-#define CALL(R_, L_) k_plaquette<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials)
+#define CALL(R_, L_) k_plaquette<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials, out, counters)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
     return cudaGetLastError();
@@ -918,9 +955,9 @@ cudaError_t Ops<N>::plaquette(int fp64, int layout, const BatchView& bv, int blo
 
 template <int N>
 cudaError_t Ops<N>::polyakov(int fp64, int layout, const BatchView& bv, int block, double* partials,
-                             cudaStream_t s)
+                             double* out, unsigned* counters, cudaStream_t s)
 {
-#define CALL(R_, L_) k_polyakov<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials)
+#define CALL(R_, L_) k_polyakov<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials, out, counters)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
     return cudaGetLastError();

@@ -64,10 +64,13 @@ template <int N> struct Ops {
                               cudaStream_t s);
     // per-CTA partials: plaquette 2 values, polyakov 2, wilson 2(R+1)(T+1),
     // unitarity 1 (max); partial layout [block][value][sum, compensation]
+    // plaquette and polyakov: with out non-null, the last CTA of each
+    // lattice also finalizes its sums into out[2 l .. 2 l + 1] (counters: one
+    // zeroed unsigned per lattice, left at zero)
     static cudaError_t plaquette(int fp64, int layout, const BatchView& bv, int block, double* partials,
-                                 cudaStream_t s);
+                                 double* out, unsigned* counters, cudaStream_t s);
     static cudaError_t polyakov(int fp64, int layout, const BatchView& bv, int block, double* partials,
-                                cudaStream_t s);
+                                double* out, unsigned* counters, cudaStream_t s);
     static cudaError_t wilson(int fp64, int layout, const BatchView& bv, int block, int R, int T,
                               double* partials, cudaStream_t s);
     static cudaError_t unitarity(int fp64, int layout, const BatchView& bv, int block, double* partials,
