@@ -178,6 +178,8 @@ int work_of(const LatDev& L, int kind)
     case WORK_HALF: return L.halfV;
     case WORK_SITES: return L.V;
     case WORK_SPATIAL: return L.X[0] * L.X[1] * L.X[2];
+    case WORK_PLANES: return plaquette_items(L.V);
+    case WORK_POLY8: return kPolyLanes * L.X[0] * L.X[1] * L.X[2];
     default: return 4 * L.V;
     }
 }
@@ -437,7 +439,7 @@ template <class F> double* group_reduce_fused(Group& g, int kind, int block, int
 
 void group_plaquette(sun_ctx* c, Group& g, double* out, cudaStream_t s)
 {
-    double* r = group_reduce_fused(g, WORK_SITES, c->blk_sites, 2, s,
+    double* r = group_reduce_fused(g, WORK_PLANES, c->blk_sites, 2, s,
                                    [&](const BatchView& v, double* part, double* out, unsigned* cnt) {
                                        OPS_CALL(g.N, plaquette, g.fp64, g.layout, v, c->blk_sites, part, out, cnt, s);
                                    });
@@ -451,7 +453,7 @@ void group_plaquette(sun_ctx* c, Group& g, double* out, cudaStream_t s)
 
 void group_polyakov(sun_ctx* c, Group& g, double* out, cudaStream_t s)
 {
-    double* r = group_reduce_fused(g, WORK_SPATIAL, c->blk_sites, 2, s,
+    double* r = group_reduce_fused(g, WORK_POLY8, c->blk_sites, 2, s,
                                    [&](const BatchView& v, double* part, double* out, unsigned* cnt) {
                                        OPS_CALL(g.N, polyakov, g.fp64, g.layout, v, c->blk_sites, part, out, cnt, s);
                                    });

@@ -587,7 +587,30 @@ SUN_DEV void load_d(const LatDev& L, const Geom& g, const int x[4], int mu, Mat<
 // Plaquette -- kernel_calc_plaquette_evenodd_cub / _normal_cub
 // (src/meas/plaquette_cub.cu:47-145): per site sum over mu < nu of
 // Re tr[U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag], nu == 3 temporal.
-// Links are widened to FP64 before the products.
+// Links are widened to FP64 before the products.  Lattices below
+// kPlaneSplitMaxV sites take one thread per (site, plane), warp-major (a
+// warp holds one plane of 32 consecutive sites, so its loads coalesce): a
+// small lattice's launch then lasts one plaquette instead of six.  Larger
+// lattices take one thread per site.  Sites are walked in lexicographic
+// order whatever the storage order, so the neighbours x + mu, x + nu that a
+// CTA reads are read by the CTAs beside it at about the same time (walking
+// one even/odd block after the other fetched every link from DRAM twice).
+template <int N, class R, int LAYOUT>
+SUN_DEV double plaquette_plane(const LatDev& L, const Geom& g, const int x[4], int mu, int nu)
+{
+    int xm[4], xn[4];
+    shifted(g, x, mu, 1, xm);
+    shifted(g, x, nu, 1, xn);
+    Mat<N, double> A, B, P, Q;
+    load_d<N, R, LAYOUT>(L, g, x, mu, A);
+    load_d<N, R, LAYOUT>(L, g, xm, nu, B);
+    mmul(A, B, P);
+    load_d<N, R, LAYOUT>(L, g, x, nu, A);
+    load_d<N, R, LAYOUT>(L, g, xn, mu, B);
+    mmul(A, B, Q);
+    return mtrace_nd(P, Q).re;
+}
+
 template <int N, class R, int LAYOUT>
 __global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partials, double* out, unsigned* counters)
 {
@@ -598,41 +621,49 @@ __global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partial
     const Geom g = geom_of(L);
     const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
     double sp = 0.0, tp = 0.0;
-    if (w < g.V) {
-        // threads walk the sites in lexicographic order whatever the storage
-        // order, so the neighbours x + mu, x + nu that a CTA reads are read by
-        // the CTAs beside it at about the same time; walking one even/odd
-        // block after the other fetched every link from DRAM twice
+    if (g.V < kPlaneSplitMaxV) {
+        const int chunk = w / 192, r = w - 192 * chunk, plane = r >> 5;
+        const int site = chunk * 32 + (r & 31);
+        if (site < g.V) {
+            const int mu = plane < 3 ? 0 : (plane < 5 ? 1 : 2);
+            const int nu = plane < 3 ? plane + 1 : (plane < 5 ? plane - 1 : 3);
+            int x[4];
+            lex_coords(g, site, x);
+            const double t = plaquette_plane<N, R, LAYOUT>(L, g, x, mu, nu);
+            if (nu == 3) tp = t; else sp = t;
+        }
+    } else if (w < g.V) {
         int x[4];
         lex_coords(g, w, x);
 #pragma unroll 1
-        for (int mu = 0; mu < 3; ++mu) {
-            int xm[4];
-            shifted(g, x, mu, 1, xm);
+        for (int mu = 0; mu < 3; ++mu)
 #pragma unroll 1
             for (int nu = mu + 1; nu < 4; ++nu) {
-                int xn[4];
-                shifted(g, x, nu, 1, xn);
-                Mat<N, double> A, B, P, Q;
-                load_d<N, R, LAYOUT>(L, g, x, mu, A);
-                load_d<N, R, LAYOUT>(L, g, xm, nu, B);
-                mmul(A, B, P);
-                load_d<N, R, LAYOUT>(L, g, x, nu, A);
-                load_d<N, R, LAYOUT>(L, g, xn, mu, B);
-                mmul(A, B, Q);
-                const double t = mtrace_nd(P, Q).re;
+                const double t = plaquette_plane<N, R, LAYOUT>(L, g, x, mu, nu);
                 if (nu == 3) tp += t; else sp += t;
             }
-        }
     }
     block_sum(sp, partials + (size_t)b * 4, sh);
     block_sum(tp, partials + (size_t)b * 4 + 2, sh);
     if (out) finalize_if_last(bv, l, partials, 2, out, counters);
 }
 
+template <int N> SUN_DEV void shfl_mat(Mat<N, double>& D, const Mat<N, double>& S, int src)
+{
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j)
+            D.e[i][j] = mkc(__shfl_sync(0xffffffffu, S.e[i][j].re, src), __shfl_sync(0xffffffffu, S.e[i][j].im, src));
+}
+
 // Polyakov loop -- kernel_calc_polyakovloop_evenodd
-// (src/meas/polyakovloop.cu:54-96): one thread per spatial site,
-// L = U_3(x,0) U_3(x,1) ... U_3(x,T-1), trace summed.
+// (src/meas/polyakovloop.cu:54-96): L = U_3(x,0) U_3(x,1) ... U_3(x,T-1),
+// trace summed over spatial sites.  kPolyLanes (8) consecutive lanes per
+// spatial site: lane k multiplies the links t in [k T / 8, (k + 1) T / 8)
+// (an empty range gives the unit matrix), then the lane products are joined
+// in order by a shuffle tree, (P0 P1)(P2 P3)..., so the time chain is T / 8
+// products plus three joins instead of T products.
 template <int N, class R, int LAYOUT>
 __global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials, double* out, unsigned* counters)
 {
@@ -643,22 +674,37 @@ __global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials
     const Geom g = geom_of(L);
     const int V3 = g.X[0] * g.X[1] * g.X[2];
     const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
-    double re = 0.0, im = 0.0;
-    if (w < V3) {
+    const int site = w / kPolyLanes, k = w - kPolyLanes * site;
+    const bool valid = site < V3;
+    Mat<N, double> P, A, T;
+    munit(P);
+    if (valid) {
         int x[4];
-        x[0] = w % g.X[0];
-        x[1] = (w / g.X[0]) % g.X[1];
-        x[2] = w / (g.X[0] * g.X[1]);
-        x[3] = 0;
-        Mat<N, double> P, A, T;
-        munit(P);
+        x[0] = site % g.X[0];
+        x[1] = (site / g.X[0]) % g.X[1];
+        x[2] = site / (g.X[0] * g.X[1]);
+        const int t0 = k * g.X[3] / kPolyLanes, t1 = (k + 1) * g.X[3] / kPolyLanes;
 #pragma unroll 1
-        for (int t = 0; t < g.X[3]; ++t) {
+        for (int t = t0; t < t1; ++t) {
             x[3] = t;
             load_d<N, R, LAYOUT>(L, g, x, 3, A);
             mmul(P, A, T);
             P = T;
         }
+    }
+    // blockDim is a multiple of 32 and of kPolyLanes: a site's lanes share a
+    // warp, every lane of the warp takes part in the shuffles
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int step = 1; step < kPolyLanes; step <<= 1) {
+        shfl_mat<N>(A, P, lane + step < 32 ? lane + step : lane);
+        if ((k & (2 * step - 1)) == 0) {
+            mmul(P, A, T);
+            P = T;
+        }
+    }
+    double re = 0.0, im = 0.0;
+    if (valid && k == 0) {
         const cx<double> tr = mtrace(P);
         re = tr.re;
         im = tr.im;

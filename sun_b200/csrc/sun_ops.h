@@ -38,7 +38,16 @@ struct InjView {
 enum UpdateMode { MODE_HB = 0, MODE_HB_INJECTED = 1, MODE_OR = 2 };
 
 // Work per lattice a launch maps CTAs onto.
-enum WorkKind { WORK_HALF = 0, WORK_SITES = 1, WORK_SPATIAL = 2, WORK_LINKS = 3 };
+// work items per lattice of a launch: half-sites, sites, spatial sites,
+// links, (site, plane) pairs of the plaquette (6 V), and 8 lanes per spatial
+// site of the Polyakov loop
+enum WorkKind { WORK_HALF = 0, WORK_SITES = 1, WORK_SPATIAL = 2, WORK_LINKS = 3, WORK_PLANES = 4, WORK_POLY8 = 5 };
+constexpr int kPolyLanes = 8;
+// lattices below this volume measure the plaquette with one thread per
+// (site, plane), warp-major (a warp: one plane of 32 consecutive sites), the
+// others with one thread per site; the choice depends on the lattice alone
+constexpr int kPlaneSplitMaxV = 1 << 17;
+__host__ __device__ inline int plaquette_items(int V) { return V < kPlaneSplitMaxV ? ((V + 31) / 32) * 192 : V; }
 
 template <int N> struct Ops {
     // one checkerboard phase (parity, mu) of heatbath or overrelaxation;
