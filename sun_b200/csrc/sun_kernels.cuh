@@ -51,12 +51,14 @@ SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
 // ---------------------------------------------------------------------------
 // Register caps of the update kernel (CTAs of 128 threads that must fit on an
 // SM).  The update is latency-bound at the register-limited occupancy.
-// Measured fastest for SU(3) on B200: overrelaxation FP32 80 registers
-// (6 CTAs, 24 warps per SM; 64 registers is no faster), heatbath FP32 102
-// registers (5 CTAs, 2.5 % faster than uncapped), overrelaxation FP64 168
-// registers (3 CTAs, 2 % faster); the FP64 heatbath is fastest uncapped.
+// Measured fastest for SU(3) on B200: overrelaxation FP32 72 registers
+// (7 CTAs, 28 warps per SM; with the phases overlapped 1.2 % faster than 80
+// registers, 6 CTAs; 64 registers is no faster), heatbath FP32 102 registers
+// (5 CTAs, 2.5 % faster than uncapped; 4 and 6 CTAs are slower),
+// overrelaxation FP64 168 registers (3 CTAs, 2 % faster); the FP64 heatbath
+// is fastest uncapped.
 #ifndef SUN_OCC_F32_OR
-#define SUN_OCC_F32_OR 6
+#define SUN_OCC_F32_OR 7
 #endif
 #ifndef SUN_OCC_F32_HB
 #define SUN_OCC_F32_HB 5
