@@ -38,6 +38,8 @@ SUN_DEV int lex_step(int lex, int xc, int Xc, int Sc, int s)
     return xc == 0 ? lex + (Xc - 1) * Sc : lex - Sc;
 }
 
+SUN_DEV int sel4(const int a[4], int i) { return i == 0 ? a[0] : (i == 1 ? a[1] : (i == 2 ? a[2] : a[3])); }
+
 // y = x shifted by s (+1/-1) along direction d (d may be a runtime value)
 SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
 {
@@ -86,9 +88,10 @@ template <class R, int MODE> struct UpdateOccupancy<3, R, MODE> {
 // Checkerboard update of the links (x, mu) with parity(x) == parity --
 // kernel_PHeatBath_evenodd (src/monte/monte.cu:44-88) and
 // kernel_overrelaxation_evenodd (src/monte/ovr.cu:41-80).  One thread per
-// half-lattice site; the staple sum keeps the reference's order (nu ascending,
-// "up" then "down"); all links are read through L2 only (LD_CG: the launch
-// overlaps the previous phase's, see the pdl note below).
+// half-lattice site; the staples are summed "up" then "down" per nu, nu in
+// the reference's ascending order for N = 6 and in the order mu+1, mu+2,
+// mu+3 (mod 4) for N <= 4 (see below); all links are read through L2 only
+// (LD_CG: the launch overlaps the previous phase's, see the pdl note below).
 template <int N, class R, int LAYOUT, int MODE>
 __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
                                                 InjView inj, int pdl)
@@ -119,23 +122,31 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)
 
     // launched as a programmatic dependent of the previous phase (pdl): that
     // phase wrote the links of direction dep = mu - 1 (mod 4), which only
-    // the staples of nu = dep read.  The staples before it in the reference's
-    // order are summed while the previous launch drains; griddepcontrol.wait
-    // then waits for it to complete, and only after that the next phase may
-    // launch (so a launch never runs beside the one two back).
+    // the staples of nu = dep read.  The staples before it are summed while
+    // the previous launch drains; griddepcontrol.wait then waits for it to
+    // complete, and only after that the next phase may launch (so a launch
+    // never runs beside the one two back).
     const int dep = pdl ? ((mu + 3) & 3) : -1;
     if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     Mat<N, R> S;
     mzero(S);
+    // N <= 4: nu = mu+1, mu+2, mu+3 (mod 4), the staple of the previous
+    // phase's direction last, so two thirds of the sum overlap the previous
+    // launch; N = 6 keeps the reference's order (nu ascending, whose FP32
+    // rounding its parity tolerance is set for)
+    constexpr bool kRot = N <= 4;
 #pragma unroll
-    for (int nu = 0; nu < 4; ++nu) {
-        if (nu == mu) continue;
+    for (int kk = kRot ? 1 : 0; kk < 4; ++kk) {
+        const int nu = kRot ? ((mu + kk) & 3) : kk;
+        if (!kRot && nu == mu) continue;
         if (nu == dep) {
             asm volatile("griddepcontrol.wait;" ::: "memory");
             asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
         }
-        const int lup = lex_step(lex, x[nu], g.X[nu], st[nu], 1);
-        const int ldn = lex_step(lex, x[nu], g.X[nu], st[nu], -1);
+        const int xn_ = kRot ? sel4(x, nu) : x[kk], Xn_ = kRot ? sel4(g.X, nu) : g.X[kk],
+                  Sn_ = kRot ? sel4(st, nu) : st[kk];
+        const int lup = lex_step(lex, xn_, Xn_, Sn_, 1);
+        const int ldn = lex_step(lex, xn_, Xn_, Sn_, -1);
         const int syp = (lup >> 1) + other;                               // x + nu
         const int sy = (ldn >> 1) + other;                                // x - nu
         const int sz = (lex_step(ldn, xm, Xm, Sm, 1) >> 1) + parity * H;  // x - nu + mu
@@ -255,15 +266,23 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
     cx<R> Sr[N];  // row r of the staple sum
 #pragma unroll
     for (int j = 0; j < N; ++j) Sr[j] = mkc<R>(0, 0);
+    // N <= 4: nu = mu+1, mu+2, mu+3 (mod 4), the staple of the previous
+    // phase's direction last, so two thirds of the sum overlap the previous
+    // launch; N = 6 keeps the reference's order (nu ascending, whose FP32
+    // rounding its parity tolerance is set for)
+    constexpr bool kRot = N <= 4;
 #pragma unroll
-    for (int nu = 0; nu < 4; ++nu) {
-        if (nu == mu) continue;
+    for (int kk = kRot ? 1 : 0; kk < 4; ++kk) {
+        const int nu = kRot ? ((mu + kk) & 3) : kk;
+        if (!kRot && nu == mu) continue;
         if (nu == dep) {
             asm volatile("griddepcontrol.wait;" ::: "memory");
             asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
         }
-        const int lup = lex_step(lex, x[nu], g.X[nu], st[nu], 1);
-        const int ldn = lex_step(lex, x[nu], g.X[nu], st[nu], -1);
+        const int xn_ = kRot ? sel4(x, nu) : x[kk], Xn_ = kRot ? sel4(g.X, nu) : g.X[kk],
+                  Sn_ = kRot ? sel4(st, nu) : st[kk];
+        const int lup = lex_step(lex, xn_, Xn_, Sn_, 1);
+        const int ldn = lex_step(lex, xn_, Xn_, Sn_, -1);
         const int syp = (lup >> 1) + other;
         const int sy = (ldn >> 1) + other;
         const int sz = (lex_step(ldn, xm, Xm, Sm, 1) >> 1) + parity * H;
