@@ -151,3 +151,23 @@ def test_batch_graph_with_one_mode(ctxs):
         Sweep(a, 1, 0, 1)
         assert np.array_equal(a.get_image(), b.get_image())
         batch.close()
+
+
+@pytest.mark.parametrize("dims,prec,lay", [((4, 4, 4, 8), "f32", 1), ((8, 8, 8, 8), "f64", 0),
+                                           ((16, 16, 16, 16), "f32", 1), ((8, 8, 8, 8), "f32", 0)])
+def test_overlapped_phases_are_deterministic(ctx, dims, prec, lay):
+    """Consecutive phases overlap (programmatic dependent launch); the same
+    passes on the same links must still give the same bits on every run --
+    a read served from a stale cache line would not."""
+    from sun_b200 import HeatBath, OverRelaxation, Sweep, gauge
+    imgs = []
+    for _ in range(3):
+        g = gauge(ctx, N=3, dims=dims, beta=6.0, atype=lay, evenodd=True, prec=prec, seed=1234)
+        g.Init(hot=True)
+        for _ in range(2):
+            HeatBath(g).Run(1)
+            OverRelaxation(g).Run(2)
+        Sweep(g, 1, 4, 2)
+        imgs.append(g.get_image())
+        g.Release()
+    assert all(np.array_equal(imgs[0], im) for im in imgs[1:])
