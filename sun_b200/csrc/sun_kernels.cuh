@@ -54,12 +54,16 @@ SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
 // ---------------------------------------------------------------------------
 // Register caps of the update kernel (CTAs of 128 threads that must fit on an
 // SM).  The update is latency-bound at the register-limited occupancy.
-// Measured fastest for SU(3) on B200: overrelaxation FP32 72 registers
-// (7 CTAs, 28 warps per SM; with the phases overlapped 1.2 % faster than 80
-// registers, 6 CTAs; 64 registers is no faster), heatbath FP32 102 registers
-// (5 CTAs, 2.5 % faster than uncapped; 4 and 6 CTAs are slower),
+// Measured fastest for SU(3) on B200, with the phases overlapped:
+// overrelaxation FP32 12-parameter 64 registers (8 CTAs, 32 warps per SM; no
+// spills; 1.2 % faster than 72 and 2.4 % than 80), FP32 full and
+// 8-parameter links 72 registers (7 CTAs; 64 spills them); heatbath FP32 102
+// registers (5 CTAs, 2.5 % faster than uncapped; 4 and 6 CTAs are slower);
 // overrelaxation FP64 168 registers (3 CTAs, 2 % faster); the FP64 heatbath
 // is fastest uncapped.
+#ifndef SUN_OCC_F32_OR12
+#define SUN_OCC_F32_OR12 8
+#endif
 #ifndef SUN_OCC_F32_OR
 #define SUN_OCC_F32_OR 7
 #endif
@@ -75,13 +79,14 @@ SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
 // N >= 4 in FP32: a 168-register cap (3 CTAs per SM) measured 18-28 % faster
 // than the uncapped kernels (208-255 registers, 1-2 CTAs) at 24^4; FP64 and
 // N = 2 are fastest uncapped.
-template <int N, class R, int MODE> struct UpdateOccupancy {
+template <int N, class R, int MODE, int LAYOUT> struct UpdateOccupancy {
     static constexpr int min_blocks = (N >= 4 && sizeof(R) == 4) ? 3 : 1;
 };
-template <class R, int MODE> struct UpdateOccupancy<3, R, MODE> {
+template <class R, int MODE, int LAYOUT> struct UpdateOccupancy<3, R, MODE, LAYOUT> {
     static constexpr bool f32 = sizeof(R) == 4;
-    static constexpr int min_blocks = MODE == MODE_OR ? (f32 ? SUN_OCC_F32_OR : SUN_OCC_F64_OR)
-                                                      : (f32 ? SUN_OCC_F32_HB : SUN_OCC_F64_HB);
+    static constexpr int min_blocks =
+        MODE == MODE_OR ? (f32 ? (LAYOUT == L_SOA12 ? SUN_OCC_F32_OR12 : SUN_OCC_F32_OR) : SUN_OCC_F64_OR)
+                        : (f32 ? SUN_OCC_F32_HB : SUN_OCC_F64_HB);
 };
 
 // ---------------------------------------------------------------------------
@@ -93,7 +98,7 @@ template <class R, int MODE> struct UpdateOccupancy<3, R, MODE> {
 // mu+3 (mod 4) for N <= 4 (see below); all links are read through L2 only
 // (LD_CG: the launch overlaps the previous phase's, see the pdl note below).
 template <int N, class R, int LAYOUT, int MODE>
-__global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE>::min_blocks)) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
+__global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE, LAYOUT>::min_blocks)) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
                                                 InjView inj, int pdl)
 {
     const int b = blockIdx.x;
