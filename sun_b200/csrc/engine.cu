@@ -193,7 +193,6 @@ struct Group {
         std::shared_ptr<DevBuf> buf;  // CTA prefix, grows only
         int nblocks = 0;
         bool valid = false;
-        bool has_map = false;  // CTA -> lattice table after the prefix
     };
     std::map<std::pair<int, int>, Begin> begins;
     DevBuf partials, out;
@@ -232,17 +231,11 @@ struct Group {
             std::vector<int> b(lats.size() + 1, 0);
             for (size_t i = 0; i < lats.size(); ++i)
                 b[i + 1] = b[i] + (work_of(lats[i]->desc, kind) + block - 1) / block;
-            // several lattices: append each CTA's lattice index, so a CTA
-            // finds its lattice with one load instead of a binary search
-            e.has_map = lats.size() > 1;
-            if (e.has_map)
-                for (size_t i = 0; i < lats.size(); ++i)
-                    for (int c = b[i]; c < b[i + 1]; ++c) b.push_back((int)i);
             if (!e.buf) e.buf = std::make_shared<DevBuf>();
             e.buf->ensure(sizeof(int) * b.size());
             ck(cudaMemcpyAsync(e.buf->p, b.data(), sizeof(int) * b.size(), cudaMemcpyHostToDevice, s), "begin upload");
             ck(cudaStreamSynchronize(s), "begin upload");
-            e.nblocks = b[lats.size()];
+            e.nblocks = b.back();
             e.valid = true;
         }
         BatchView v;
@@ -250,7 +243,6 @@ struct Group {
         v.begin = reinterpret_cast<const int*>(e.buf->p);
         v.nlat = (int)lats.size();
         v.nblocks = e.nblocks;
-        v.lat_of = e.has_map ? v.begin + lats.size() + 1 : nullptr;
         return v;
     }
 };

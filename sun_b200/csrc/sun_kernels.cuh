@@ -13,7 +13,6 @@ namespace sunb {
 
 SUN_DEV int find_lat(const BatchView& bv, int b)
 {
-    if (bv.lat_of) return __ldg(bv.lat_of + b);
     int lo = 0, hi = bv.nlat - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;

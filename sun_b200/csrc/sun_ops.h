@@ -25,7 +25,6 @@ struct BatchView {
     const int* begin;
     int nlat;
     int nblocks;
-    const int* lat_of = nullptr;  // lattice of each CTA (several lattices), or null
 };
 
 // Uniforms injected per link for oracle parity: link (lex, mu) reads
