@@ -5,9 +5,10 @@
 // oracle/ref/Makefile with shim_inject/ first on the include path.
 //
 // usage: ref_link_probe {hb|or|reunit} IN OUT beta
-// IN : int32 nlinks, int32 stride; double U[nlinks][9][2]; double F[nlinks][9][2];
+// IN : int32 nlinks, int32 stride; double U[nlinks][NC*NC][2]; double F[nlinks][NC*NC][2];
 //      double u[nlinks][stride]   (F is the staple^dagger the update receives)
-// OUT: double U'[nlinks][9][2]; int32 used[nlinks] (uniforms consumed, -1 overrun)
+// OUT: double U'[nlinks][NC*NC][2]; int32 used[nlinks] (uniforms consumed, -1 overrun)
+// NC = NCOLORS of the build (3, or 4 and 6 for the builds of `make ncolors`).
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -30,13 +31,14 @@ __global__ void k_link(const double* U, const double* F, const double* u, int st
                        int* flags)
 {
     typedef double Real;
+    constexpr int NC = NCOLORS, NE = NCOLORS * NCOLORS;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     msun A, B;
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) {
-            A.e[a][b] = complex::make_complex(U[(i * 9 + a * 3 + b) * 2], U[(i * 9 + a * 3 + b) * 2 + 1]);
-            B.e[a][b] = complex::make_complex(F[(i * 9 + a * 3 + b) * 2], F[(i * 9 + a * 3 + b) * 2 + 1]);
+    for (int a = 0; a < NC; ++a)
+        for (int b = 0; b < NC; ++b) {
+            A.e[a][b] = complex::make_complex(U[(i * NE + a * NC + b) * 2], U[(i * NE + a * NC + b) * 2 + 1]);
+            B.e[a][b] = complex::make_complex(F[(i * NE + a * NC + b) * 2], F[(i * NE + a * NC + b) * 2 + 1]);
         }
     cuRNGState st;
     st.u = u + (size_t)i * stride;
@@ -46,10 +48,10 @@ __global__ void k_link(const double* U, const double* F, const double* u, int st
     if (MODE == 0) heatBathSUN<Real>(A, B, st);
     else if (MODE == 1) overrelaxationSUN<Real>(A, B);
     else reunit_link<Real>(&A);
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) {
-            out[(i * 9 + a * 3 + b) * 2] = A.e[a][b].real();
-            out[(i * 9 + a * 3 + b) * 2 + 1] = A.e[a][b].imag();
+    for (int a = 0; a < NC; ++a)
+        for (int b = 0; b < NC; ++b) {
+            out[(i * NE + a * NC + b) * 2] = A.e[a][b].real();
+            out[(i * NE + a * NC + b) * 2 + 1] = A.e[a][b].imag();
         }
     used[i] = flags[i] ? -1 : st.pos;
 }
@@ -66,7 +68,7 @@ int main(int argc, char** argv)
     if (!f) return 3;
     int n = 0, stride = 0;
     if (fread(&n, 4, 1, f) != 1 || fread(&stride, 4, 1, f) != 1) return 3;
-    std::vector<double> U(n * 18), F(n * 18), u((size_t)n * stride);
+    std::vector<double> U((size_t)n * 2 * NCOLORS * NCOLORS), F((size_t)n * 2 * NCOLORS * NCOLORS), u((size_t)n * stride);
     if (fread(U.data(), 8, U.size(), f) != U.size() || fread(F.data(), 8, F.size(), f) != F.size() ||
         fread(u.data(), 8, u.size(), f) != u.size())
         return 3;
