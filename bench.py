@@ -137,6 +137,53 @@ def cpu_sample(nthreads=0, reps=1, lattice=None):
     return reps * 5 * (V // 2) / dt, threads, dt
 
 
+def lockstep(g, nsweeps, n_hb=1, n_or=4, flip=1e-3):
+    """Plaquette error of the engine's sweeps against the FP64 oracle, in
+    lockstep: before each sweep the oracle takes the engine's stored links,
+    then both run the same sweep with the same Philox draws (24-bit uniforms
+    for FP32 lattices), the oracle in FP64 arithmetic.  Per sweep: the signed
+    difference of the mean plaquette (engine - oracle) and the number of
+    links that differ by more than `flip`: where a heatbath accept/reject
+    decision went the other way at the rounding boundary, the following
+    overrelaxation passes of the sweep spread the difference over a region
+    around that link.  g must have reunit_every = 0.
+    The dynamics is chaotic, so only this one-sweep error is a precision
+    figure; longer chains agree in distribution, not link by link."""
+    import numpy as np
+    from oracle import oracle as O
+    from sun_b200 import PlaquetteCUB, Sweep
+    X = list(g.dims)
+    fp32 = g.prec == "f32"
+    diffs, off = [], []
+    for _ in range(nsweeps):
+        U = g.Get()
+        seed, hb, _sw = g.rng_state()
+        Sweep(g, n_hb, n_or, 1)
+        p = PlaquetteCUB(g).Run()
+        O.sweeps(U, X, g.beta, n_hb, n_or, 1, mode=O.RNG_PHILOX32 if fp32 else O.RNG_PHILOX64, seed=seed, pass_=hb)
+        po = O.plaquette(U, X)
+        d = np.abs(g.Get() - U).reshape(U.shape[0] * 4, -1).max(axis=1)
+        off.append(int((d > flip).sum()))
+        diffs.append(0.5 * (p.real + p.imag) - 0.5 * (po[0] + po[1]))
+        del U, d
+    a = np.abs(diffs)
+    return {"sweeps": nsweeps, "abs_diff_max": float(a.max()), "abs_diff_mean": float(a.mean()),
+            "signed_diff_mean": float(np.mean(diffs)), "signed_diffs": [float(v) for v in diffs],
+            "links_off_per_sweep": off, "flip_threshold": flip}
+
+
+def lockstep_copy(g, nsweeps):
+    """lockstep() on a copy of g (same links and RNG counters, no
+    reunitarization inside the window); g itself is left as it was."""
+    from sun_b200 import gauge
+    c = gauge(g.ctx, N=g.N, dims=g.dims, beta=g.beta, atype=g.atype, evenodd=True, prec=g.prec, seed=g.seed,
+              reunit_every=0)
+    c.Copy(g)
+    out = lockstep(c, nsweeps)
+    c.Release()
+    return out
+
+
 def accuracy_report(ctx, g, stream):
     """Accuracy of the FP32 12-parameter sweep against the FP64 oracle:
     (1) max |U^dagger U - 1| of the benchmarked lattice after its sweeps
@@ -166,6 +213,13 @@ def accuracy_report(ctx, g, stream):
     out["one_sweep_from_haar"] = {"plaquette_f32_gpu": [p1.real, p1.imag], "plaquette_f64_oracle": [po1[0], po1[1]],
                                   "abs_diff": max(abs(p1.real - po1[0]), abs(p1.imag - po1[1])),
                                   "draws": "the same Philox stream (24-bit uniforms) on both sides"}
+    # lockstep from the benchmarked (thermalized) configuration: a copy with
+    # the same links and RNG counters, no reunitarization inside the window
+    gl = gauge(ctx, N=N, dims=DIMS, beta=BETA, atype=1, evenodd=True, prec="f32", seed=SEED, reunit_every=0)
+    gl.Copy(g)
+    out["lockstep"] = lockstep(gl, 10)
+    out["lockstep"]["from"] = "the benchmarked configuration after its sweeps (thermalized, beta = 6.0)"
+    gl.Release()
     return out
 
 
@@ -221,7 +275,42 @@ def run_reference(args):
                                    "over the full 32^4 lattice, FP64 oracle, OpenMP over sites"},
         "e2e": {"value": value, "unit": "link-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    line["reference_gpu"] = reference_gpu_timing()
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_timing(sweeps=20):
+    """The reference's own build (oracle/_ref/ref_probe: the reference
+    compiled from its sources for sm_100a) timed on this GPU through its
+    public API -- HeatBath::Run + 4 x OverRelaxation::Run per sweep, its
+    autotuner on, CUDA events -- on the benchmark lattice in the FP32
+    12-parameter layout and in FP64 full links, with the SM clocks sampled
+    meanwhile.  A report beside the CPU value, not the arm's value."""
+    probe = os.path.join(ROOT, "oracle", "_ref", "ref_probe")
+    if not os.path.exists(probe):
+        return {"unavailable": "oracle/_ref/ref_probe not built (the reference sources were absent at build time)"}
+    out = {"what": f"reference build, SU(3) {'x'.join(map(str, DIMS))} beta={BETA}, cold start, 3 untimed sweeps "
+                   f"(autotuning), {sweeps} timed sweeps of 1 HB + 4 OR", "sweeps": sweeps}
+    with tempfile.TemporaryDirectory() as tmp:
+        env = dict(os.environ, SUN_REF_TUNE="1", CULQCD_RESOURCE_PATH=tmp)
+        clocks = ClockSampler(0)
+        clocks.start()
+        for kind in ("f32soa12", "f64soa"):
+            try:
+                r = subprocess.run([probe, "timing"] + [str(d) for d in DIMS] + [repr(BETA), str(sweeps), kind],
+                                   capture_output=True, text=True, timeout=600, env=env)
+            except Exception as e:  # noqa: BLE001
+                out[kind] = {"unavailable": f"{type(e).__name__}: {e}"}
+                continue
+            f = [l.split() for l in r.stdout.splitlines() if l.startswith("timing")]
+            if r.returncode != 0 or not f:
+                out[kind] = {"unavailable": f"rc={r.returncode}: {r.stderr.strip()[-200:]}"}
+                continue
+            v = dict(zip(f[0][1::2], (float(x) for x in f[0][2::2])))
+            out[kind] = {"value": v["link_updates_per_s"], "unit": "link-updates/s", "sweep_ms": v["sweep_ms"],
+                         "hb_ms_per_pass": v["hb_ms_per_pass"], "or_ms_per_pass": v["or_ms_per_pass"]}
+        out["clocks"] = clocks.stop()
+    return out
 
 
 def e2e_pipeline(torch, L, ctx, g0, host0, steps, barrier, max_over_ranks):
@@ -290,10 +379,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 and batched side measurements")
+    ap.add_argument("--profile-case", default=None,
+                    help="run one short workload for a profiler and exit: suN_L (SU(N), L^4, FP32 links, hot "
+                         "start, one sweep of 1 HB + 4 OR), e.g. su6_20")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_case:
+        return profile_case(args.profile_case)
 
     import torch
     world, rank, local = dist_setup()
@@ -409,9 +503,9 @@ def main():
         extras["fp64_soa_plain"] = {"value": 20 * V * k64 / t64, "unit": "link-updates/s", "sweeps": k64,
                                     "hbm_gbs_model": 20 * V * k64 * 9 * 144 / t64 / 1e9}
         g64.Release()
-        extras["batched"] = batched_bench(ctx, L, sp, stream, args)
+        extras["batched"] = batched_bench(ctx, L, sp, stream, args, accuracy=rank == 0 and not args.no_cpu)
         extras["plain_small_fp64"] = plain_small_bench(ctx, L, sp, stream)
-        extras["sun_n"] = sun_n_bench(ctx, L, sp, stream)
+        extras["sun_n"] = sun_n_bench(ctx, L, sp, stream, accuracy=rank == 0 and not args.no_cpu)
         extras["smearing"] = smear_bench(ctx, L, sp, stream)
         if rank == 0:
             extras["serving"] = serving_bench(ctx)
@@ -421,6 +515,8 @@ def main():
             extras["serving"]["light_load"] = {k: light[k] for k in ("jobs", "completed", "arrival_rate_per_s",
                                                                       "window_s", "p50_latency_s", "p99_latency_s",
                                                                       "link_updates_per_s", "wall_s")}
+            if not args.no_cpu:
+                extras["serving"]["accuracy"] = serving_accuracy(ctx)
 
     line = {
         "metric": "link-updates/s",
@@ -455,6 +551,16 @@ def main():
                         "unit": "GB/s", "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind,
                         "launch_us": t_or * 1e6, "algorithmic_bytes_per_launch": bytes_or,
                         "hb_launch_us": t_hb * 1e6, "hb_achieved_gbs": bytes_or / t_hb / 1e9}
+    # the reference's own, larger byte model beside the compulsory one: 20
+    # link-records of 12 FP32 reals per update (OverRelaxation::bytes,
+    # src/monte/ovr.cu:254-259; the heatbath adds two 48 B cuRAND states,
+    # monte.cu:258-262, which a Philox stream does not have)
+    bytes_ref = (V // 2) * 20 * 12 * 4
+    line["roofline"]["reference_model"] = {
+        "bytes_per_update": 20 * 12 * 4, "achieved": bytes_ref / t_or / 1e9, "unit": "GB/s",
+        "frac": bytes_ref / t_or / 1e9 / peak,
+        "note": "20 link-records per update counted as if every staple load came from DRAM; the compulsory model "
+                "above (9 records) is the roofline"}
     line["e2e"] = {"value": world * 20 * V * k_e2e / t_e2e, "unit": "link-updates/s",
                    "h2d_bytes_per_step": img_bytes, "d2h_bytes_per_step": img_bytes,
                    "step": "four host-resident lattices in rotation: upload image (pinned) + 1 sweep + download "
@@ -487,6 +593,24 @@ def main():
     ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def profile_case(case):
+    """A short workload for a profiler (ncu): SU(N) on L^4, FP32 links (the
+    benchmark's 12-parameter layout for SU(3), full links otherwise), hot
+    start, one sweep of 1 heatbath + 4 overrelaxation passes (8 heatbath
+    then 32 overrelaxation update launches)."""
+    import torch
+    from sun_b200 import Context, Sweep, gauge
+    n, l = case[2:].split("_")
+    with Context(0) as ctx:
+        g = gauge(ctx, N=int(n), dims=(int(l),) * 4, beta={2: 2.5, 3: 6.0, 4: 11.1, 6: 25.0}[int(n)],
+                  atype=1 if int(n) == 3 else 0, evenodd=True, prec="f32", seed=SEED)
+        g.Init(hot=True)
+        Sweep(g, 1, 4, 1)
+        torch.cuda.synchronize()
+        g.Release()
+    print(f"profile case {case}: one sweep done", flush=True)
 
 
 def serving_jobs(rate=50.0, window=4.0, seed=1234):
@@ -553,7 +677,29 @@ def serving_bench(ctx, rate=50.0, window=3.0, max_active=256):
     return out
 
 
-def batched_bench(ctx, L, sp, stream, args):
+def serving_accuracy(ctx):
+    """Plaquette error against the FP64 oracle of one served job per N: the
+    first job of each N in the stream is run alone (a job's result does not
+    depend on its batch mates), then one lockstep sweep from its final
+    configuration."""
+    from sun_b200 import SOA, SOA12, Sweep, gauge
+    out = {}
+    for j in serving_jobs():
+        key = f"su{j['N']}"
+        if key in out:
+            continue
+        g = gauge(ctx, N=j["N"], dims=j["dims"], beta=j["beta"], atype=SOA12 if j["N"] == 3 else SOA,
+                  evenodd=True, prec="f32", seed=j["seed"], reunit_every=10)
+        g.Init(hot=True)
+        Sweep(g, 1, 4, j["sweeps"])
+        r = lockstep_copy(g, 1)
+        out[key] = {"dims": list(j["dims"]), "sweeps": j["sweeps"], "abs_diff": r["abs_diff_max"],
+                    "links_off_by_1e-3": r["links_off_per_sweep"][0]}
+        g.Release()
+    return out
+
+
+def batched_bench(ctx, L, sp, stream, args, accuracy=False):
     """64 independent SU(3) lattices, L in {8,12,16}, T in {L,2L}, beta in
     [5.7,6.4], FP32 SOA12, advanced together from a captured CUDA graph."""
     import numpy as np
@@ -585,6 +731,14 @@ def batched_bench(ctx, L, sp, stream, args):
     rate = 20 * vol * k / t
     out = {"value": rate, "unit": "link-updates/s", "lattices": 64, "total_sites": vol, "sweeps": k,
            "hbm_gbs_model": rate * 9 * 48 / 1e9, "graph": True}
+    if accuracy:
+        # plaquette error against the FP64 oracle, one lockstep sweep from the
+        # final configuration of three of the lattices
+        out["accuracy"] = []
+        for i in (0, 21, 42):
+            r = lockstep_copy(lats[i], 1)
+            out["accuracy"].append({"lattice": i, "dims": list(lats[i].dims), "abs_diff": r["abs_diff_max"],
+                                    "links_off_by_1e-3": r["links_off_per_sweep"][0]})
     b.close()
     for g in lats:
         g.Release()
@@ -626,11 +780,28 @@ def plain_small_bench(ctx, L, sp, stream, sweeps=200):
            "lattice": list(dims), "precision": "f64", "layout": "SOA", "start": "cold",
            "final_plaquette": [pl[0], pl[1]], "final_polyakov": [po[0], po[1]],
            "measure": "plaquette + Polyakov loop to the host every sweep"}
+    # the same sweeps and per-sweep measurements in one call
+    # (sun_sweep_measure: one captured graph of sweep + plaquette + Polyakov
+    # loop replayed back to back, the observables copied once at the end)
+    import numpy as np
+    pp, pq = np.zeros(2 * sweeps), np.zeros(2 * sweeps)
+    dp = C.POINTER(C.c_double)
+    check(L.sun_sweep_measure(g.h, 1, 4, 3, pp.ctypes.data_as(dp), pq.ctypes.data_as(dp), sp), ctx.h)
+    g.Init(hot=False)
+    stream.synchronize()
+    e0.record(stream)
+    check(L.sun_sweep_measure(g.h, 1, 4, sweeps, pp.ctypes.data_as(dp), pq.ctypes.data_as(dp), sp), ctx.h)
+    e1.record(stream)
+    stream.synchronize()
+    t1 = e0.elapsed_time(e1) / 1e3
+    out["one_call"] = {"value": 20 * V * sweeps / t1, "ms_per_sweep": 1e3 * t1 / sweeps,
+                       "final_plaquette": [pp[-2], pp[-1]], "final_polyakov": [pq[-2], pq[-1]],
+                       "same_as_per_sweep_calls": bool(pp[-2] == pl[0] and pp[-1] == pl[1] and pq[-2] == po[0])}
     g.Release()
     return out
 
 
-def sun_n_bench(ctx, L, sp, stream, sweeps=10):
+def sun_n_bench(ctx, L, sp, stream, sweeps=10, accuracy=False):
     """SU(N), N in {2, 4, 6}, on 24^4 with beta/(2 N^2) fixed (2.5, 11.1,
     25.0): FP32 full links, FP64 compensated reductions, hot start; a bounded
     sample of `sweeps` timed sweeps of 1 HB + 4 OR after 2 warm-up sweeps, then
@@ -660,6 +831,12 @@ def sun_n_bench(ctx, L, sp, stream, sweeps=10):
         out[f"su{n}"] = {"value": rate, "unit": "link-updates/s", "beta": beta, "sweeps": sweeps,
                          "hbm_frac": rate * 9 * 8 * n * n / 1e9 / peak, "plaquette": [pl[0], pl[1]],
                          "wilson_4x4_re": [[round(float(v), 8) for v in row] for row in w.real]}
+        if accuracy:
+            r = lockstep_copy(g, 1)
+            out[f"su{n}"]["accuracy"] = {"abs_diff": r["abs_diff_max"],
+                                         "links_off_by_1e-3": r["links_off_per_sweep"][0],
+                                         "how": "one lockstep sweep from the final configuration against the "
+                                                "FP64 oracle"}
         g.Release()
     out["lattice"] = list(dims)
     out["bytes_per_update"] = "9 link-records of 8 N^2 B (FP32 full links)"

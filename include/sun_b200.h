@@ -80,6 +80,9 @@ typedef struct {
 sun_status sun_init(const sun_config *cfg, sun_ctx **out);
 sun_status sun_finalize(sun_ctx *ctx);
 const char *sun_last_error_string(const sun_ctx *ctx);
+/* the context's device-memory admission budget: sun_config.hbm_budget_bytes,
+ * or 90% of the free memory at sun_init; servers admit jobs against it */
+sun_status sun_ctx_hbm_budget(const sun_ctx *ctx, size_t *bytes);
 const char *sun_version(void);
 /* host-side fault injection for tests (no reference counterpart): after
  * after_n more device allocations succeed, every further one reports
@@ -110,6 +113,12 @@ sun_status sun_lattice_upload_async(sun_lattice *lat, const void *host_image, vo
 sun_status sun_lattice_download_async(sun_lattice *lat, void *host_image, void *stream);
 /* layout / order / precision conversion, gauge::Copy (src/gaugearray.cu:130) */
 sun_status sun_lattice_copy(sun_lattice *dst, sun_lattice *src, void *stream);
+/* Sweep limit (no reference counterpart): once the lattice's sweep counter
+ * reaches `limit`, sweeps leave it unchanged -- the update launches skip it,
+ * its counters and its reunitarization schedule stop -- so a batch can run
+ * more sweeps than some of its lattices need and each still ends after
+ * exactly its own count.  0 (the default) means no limit. */
+sun_status sun_lattice_set_sweep_limit(sun_lattice *lat, uint32_t limit);
 /* RNG state for checkpoint: RNG::Save / RNG::Read (src/random.cu:164, :183);
  * with Philox the state is (seed, heatbath-pass counter, sweep counter) */
 sun_status sun_lattice_get_rng(sun_lattice *lat, uint64_t *seed, uint32_t *hb_passes, uint32_t *sweeps);
@@ -123,9 +132,30 @@ sun_status sun_overrelax(sun_lattice *lat, int n_passes, void *stream);
 /* n_sweeps x (n_hb heatbath + n_or overrelaxation); reunitarizes after every
  * reunit_every-th sweep (lattice parameter) */
 sun_status sun_sweep(sun_lattice *lat, int n_hb, int n_or, int n_sweeps, void *stream);
+/* n_sweeps sweeps of (n_hb heatbath + n_or overrelaxation) with the
+ * plaquette and the Polyakov loop measured after every sweep -- the
+ * reference driver's loop of HeatBath::Run, OverRelaxation::Run,
+ * PlaquetteCUB::Run and OnePolyakovLoop::Run (src/monte/monte.cu:196,
+ * src/monte/ovr.cu:182, src/meas/plaquette_cub.cu:226,
+ * src/meas/polyakovloop.cu:637) in one call, with the same results as
+ * sun_sweep + sun_plaquette + sun_polyakov per sweep.  plaq[2i], plaq[2i+1]:
+ * spatial and temporal plaquette after sweep i; poly[2i], poly[2i+1]:
+ * Polyakov loop; host arrays of 2 n_sweeps doubles, either may be NULL. */
+sun_status sun_sweep_measure(sun_lattice *lat, int n_hb, int n_or, int n_sweeps, double *plaq, double *poly,
+                             void *stream);
 /* one heatbath pass fed caller uniforms (oracle parity): device buffer
  * u[(lex*4 + mu)*stride + k]; running out sets SUN_ERR_DEVICE_FLAG */
 sun_status sun_heatbath_injected(sun_lattice *lat, const double *dev_uniforms, int stride, void *stream);
+
+/* Test hook (no reference counterpart): n draws of the SU(2) heatbath
+ * element for a fixed alpha on the current device, in the given arithmetic,
+ * exactly as the update kernels make them -- the restatement of
+ * generate_su2_matrix_milc (include/device_PHB_OVR.h:163-223): Kennedy-Pendleton
+ * for alpha > 2, Creutz otherwise, 20 retries.  Draw i reads the Philox
+ * stream (seed, i, 0, pass 0).  out: host buffer of 4 n doubles
+ * (a0, a1, a2, a3) per draw; 0 < n <= 2^26.  Errors through
+ * sun_last_error_string(NULL). */
+sun_status sun_debug_su2_draws(sun_precision prec, double alpha, uint64_t seed, int n, double *out);
 
 /* ---- Reunitarize<Real>::Run (src/reunitarize.cu:78), FP64 arithmetic ---- */
 sun_status sun_reunitarize(sun_lattice *lat, void *stream);
@@ -155,7 +185,9 @@ sun_status sun_plaquette(sun_lattice *lat, double out[2], void *stream);
  * 2 doubles {spatial, temporal}, written asynchronously on `stream`.  The
  * first call on each device looks up the scratch address (no allocation);
  * make that first call before any stream capture.  All calls share the
- * scratch: calls that overlap on the GPU race.  Errors: status code plus
+ * scratch: calls that overlap on the GPU race.  The looked-up address is kept
+ * for the process's life: after cudaDeviceReset on a device, do not call this
+ * entry point on that device again.  Errors: status code plus
  * sun_last_error_string(NULL). */
 sun_status sun_plaquette_noalloc(const void *d_links, const sun_lattice_params *p, double *d_out, void *stream);
 sun_status sun_polyakov(sun_lattice *lat, double out[2], void *stream);
@@ -215,6 +247,10 @@ sun_status sun_batch_sweep(sun_batch *b, int n_hb, int n_or, int n_sweeps, int u
 /* out[2*i], out[2*i+1] for the i-th lattice in insertion order */
 sun_status sun_batch_plaquette(sun_batch *b, double *out, void *stream);
 sun_status sun_batch_polyakov(sun_batch *b, double *out, void *stream);
+/* WilsonLoop (src/meas/wilsonloop.cu:535) of every lattice, one launch per
+ * class: out[(i (R+1)(T+1) + t + r (T+1)) * 2 + {0, 1}] for the i-th lattice
+ * in insertion order; R, T below every lattice's extents, at most 8 */
+sun_status sun_batch_wilson_loops(sun_batch *b, int R, int T, double *out, void *stream);
 
 /* ---- continuous-batching server ---- */
 typedef struct {
@@ -246,13 +282,16 @@ sun_status sun_server_create(sun_ctx *ctx, int max_active, sun_server **out);
 sun_status sun_server_destroy(sun_server *s);
 /* queue a job; the server admits it when its HBM footprint fits */
 sun_status sun_server_submit(sun_server *s, const sun_job *job, int64_t *id);
-/* run one scheduling step: admit, advance every active job by one sweep,
- * retire finished jobs; *n_done results are written to out[0..cap) */
+/* run one scheduling step: admit queued jobs, advance every active job by up
+ * to K sweeps (K sized so a step is ~50 ms of GPU work, at most 16; each job
+ * stops at its own sweep count, sun_lattice_set_sweep_limit), measure the
+ * finished jobs in batched launches and retire them; *n_done results are
+ * written to out[0..cap) */
 sun_status sun_server_step(sun_server *s, sun_result *out, int cap, int *n_done);
 sun_status sun_server_pending(const sun_server *s, int *queued, int *active);
 /* bytes a job needs on the device (links + measurement scratch) */
 sun_status sun_job_footprint(const sun_job *job, size_t *bytes);
-/* override the admission budget (default 85% of free device memory) */
+/* override the admission budget (default: the context's, sun_ctx_hbm_budget) */
 sun_status sun_server_set_budget(sun_server *s, size_t bytes);
 /* the admission rule: how many of the queued jobs (FIFO, footprints given)
  * to admit with `free_slots` slots and `used` of `budget` bytes taken */

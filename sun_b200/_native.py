@@ -67,14 +67,18 @@ _SIGS = {
     "sun_lattice_download_async": [_vp, _vp, _vp],
     "sun_lattice_get_rng": [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
     "sun_lattice_set_rng": [_vp, C.c_uint64, C.c_uint32, C.c_uint32],
+    "sun_lattice_set_sweep_limit": [_vp, C.c_uint32],
+    "sun_ctx_hbm_budget": [_vp, C.POINTER(C.c_size_t)],
     "sun_heatbath": [_vp, C.c_int, _vp],
     "sun_overrelax": [_vp, C.c_int, _vp],
     "sun_sweep": [_vp, C.c_int, C.c_int, C.c_int, _vp],
+    "sun_sweep_measure": [_vp, C.c_int, C.c_int, C.c_int, _dp, _dp, _vp],
     "sun_heatbath_injected": [_vp, _vp, C.c_int, _vp],
     "sun_reunitarize": [_vp, _vp],
     "sun_unitarity_violation": [_vp, _dp, _vp],
     "sun_link_trace_det": [_vp, _dp, _vp],
     "sun_debug_fail_allocations": [C.c_int],
+    "sun_debug_su2_draws": [C.c_int, C.c_double, C.c_uint64, C.c_int, _dp],
     "sun_plaquette": [_vp, _dp, _vp],
     "sun_plaquette_noalloc": [_vp, C.POINTER(SunLatticeParams), _vp, _vp],
     "sun_polyakov": [_vp, _dp, _vp],
@@ -94,6 +98,7 @@ _SIGS = {
     "sun_batch_sweep": [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp],
     "sun_batch_plaquette": [_vp, _dp, _vp],
     "sun_batch_polyakov": [_vp, _dp, _vp],
+    "sun_batch_wilson_loops": [_vp, C.c_int, C.c_int, _dp, _vp],
     "sun_server_create": [_vp, C.c_int, C.POINTER(_vp)],
     "sun_server_destroy": [_vp],
     "sun_server_submit": [_vp, C.POINTER(SunJob), C.POINTER(C.c_int64)],

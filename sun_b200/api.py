@@ -159,6 +159,11 @@ class gauge:
         check(lib().sun_lattice_get_rng(self.h, C.byref(s), C.byref(h), C.byref(w)), self.ctx.h)
         return s.value, h.value, w.value
 
+    def set_sweep_limit(self, limit: int) -> None:
+        """Sweeps leave the lattice unchanged once its sweep counter reaches
+        `limit` (0: no limit)."""
+        check(lib().sun_lattice_set_sweep_limit(self.h, int(limit)), self.ctx.h)
+
     def set_rng_state(self, seed: int, hb_passes: int, sweeps: int) -> None:
         check(lib().sun_lattice_set_rng(self.h, seed, hb_passes, sweeps), self.ctx.h)
         self.seed = seed
@@ -187,6 +192,18 @@ class OverRelaxation:
 
 def Sweep(g: gauge, n_hb: int = 1, n_or: int = 4, n_sweeps: int = 1) -> None:
     check(lib().sun_sweep(g.h, n_hb, n_or, n_sweeps, None), g.ctx.h)
+
+
+def SweepMeasure(g: gauge, n_hb: int = 1, n_or: int = 4, n_sweeps: int = 1):
+    """n_sweeps sweeps with the plaquette and Polyakov loop after each:
+    returns (plaquette [n_sweeps, 2] {spatial, temporal}, Polyakov loop
+    [n_sweeps] complex)."""
+    pl = np.zeros(2 * n_sweeps)
+    po = np.zeros(2 * n_sweeps)
+    dp = C.POINTER(C.c_double)
+    check(lib().sun_sweep_measure(g.h, n_hb, n_or, n_sweeps, pl.ctypes.data_as(dp), po.ctypes.data_as(dp), None),
+          g.ctx.h)
+    return pl.reshape(n_sweeps, 2), po[0::2] + 1j * po[1::2]
 
 
 class Reunitarize:
@@ -347,6 +364,14 @@ class Batch:
         o = np.zeros(2 * len(self.members))
         check(lib().sun_batch_plaquette(self.h, o.ctypes.data_as(C.POINTER(C.c_double)), None), self.ctx.h)
         return o.reshape(-1, 2)
+
+    def wilson_loops(self, R: int, T: int) -> np.ndarray:
+        """W(r, t) of every lattice: complex [n, R + 1, T + 1]."""
+        n = len(self.members)
+        out = np.zeros(n * 2 * (R + 1) * (T + 1))
+        check(lib().sun_batch_wilson_loops(self.h, R, T, out.ctypes.data_as(C.POINTER(C.c_double)), None), self.ctx.h)
+        o = out.reshape(n, R + 1, T + 1, 2)
+        return o[..., 0] + 1j * o[..., 1]
 
     def polyakov(self) -> np.ndarray:
         o = np.zeros(2 * len(self.members))

@@ -20,9 +20,13 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libsun_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
+# -fmad=false: no implicit multiply-add contraction; the kernels write out
+# every fused operation (sun_math.cuh), so equal source arithmetic rounds
+# equally in every kernel
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr",
               "-I" + os.path.join(ROOT, "include")] + ARCH
-UNITS = ["ops_n2.cu", "ops_n3.cu", "ops_n4.cu", "ops_n6.cu", "engine.cu", "server.cu", "noalloc.cu"]
+UNITS = ["ops_n2.cu", "ops_n3.cu", "ops_n4.cu", "ops_n6.cu", "engine.cu", "server.cu", "noalloc.cu",
+         "draw_check.cu"]
 
 
 def _nvcc() -> str:

@@ -129,7 +129,8 @@ struct sun_ctx {
     // launch shapes (CTA sizes) per kernel family
     int blk_update = 128, blk_sites = 128, blk_links = 256, blk_wilson = 64;
     // update kernel: 0 chosen by size (or by the tuner), 1 always one thread
-    // per half-site (k_update), 2 always N lanes per half-site (k_update_rows).
+    // per half-site (k_update), 2 always N lanes per half-site (k_update_rows),
+    // 3 the tiled kernel where it applies (k_update_tile: N >= 4, full links).
     // By size: groups of N >= 4, and of SU(3) with FP64 full links, with at
     // most rows_max_halfv half-sites (FP64: half that) take the row-split
     // kernel.  Sweeps measured on B200: SU(6) 8^4 FP32 3.1x and FP64 2.2x
@@ -155,7 +156,7 @@ struct sun_lattice {
     sun_ctx* ctx = nullptr;
     sun_lattice_params p{};
     DevBuf links;
-    DevBuf state;        // uint32 [heatbath passes, sweeps]
+    DevBuf state;        // uint32 [heatbath passes, sweeps, advanced, spare]
     size_t bytes = 0;
     LatDev desc{};
     unsigned version = 0;    // bumped when desc changes (device tables re-upload)
@@ -165,6 +166,15 @@ struct sun_lattice {
     cudaGraphExec_t sweep_graph = nullptr;
     int graph_hb = -1, graph_or = -1;
     unsigned graph_version = 0;
+    // one sweep plus the plaquette and the Polyakov loop as a CUDA graph,
+    // replayed by sun_sweep_measure: the measurement kernels write row *slot
+    // of meas (meas_rows rows of plaquettes, then as many of Polyakov loops)
+    // and the graph advances slot
+    cudaGraphExec_t meas_graph = nullptr;
+    int meas_hb = -1, meas_or = -1;
+    unsigned meas_version = 0;
+    size_t meas_rows = 0;
+    DevBuf meas, slot;
     ~sun_lattice();
 };
 
@@ -263,8 +273,14 @@ struct Group {
 // -- sweeps ------------------------------------------------------------------
 // Launch shape of the update: cfg > 0 runs k_update with CTAs of cfg threads
 // (one per half-site), cfg < 0 runs k_update_rows with CTAs of -cfg threads
-// (N lanes per half-site, 32/N half-sites per warp).  Both give the same bits.
-int upd_sites_per_cta(int N, int cfg) { return cfg > 0 ? cfg : (-cfg / 32) * (32 / N); }
+// (N lanes per half-site, 32/N half-sites per warp), cfg == kCfgTile runs
+// k_update_tile (N warps per 32 half-sites, N >= 4).  All give the same bits.
+constexpr int kCfgTile = 1 << 20;
+int upd_sites_per_cta(int N, int cfg)
+{
+    return cfg == kCfgTile ? 32 : (cfg > 0 ? cfg : (-cfg / 32) * (32 / N));
+}
+bool tile_ok(const Group& g) { return g.N >= 4 && g.layout == SUN_SOA; }
 
 BatchView upd_view(Group& g, int cfg, cudaStream_t s) { return g.view(WORK_HALF, upd_sites_per_cta(g.N, cfg), s); }
 
@@ -273,7 +289,8 @@ BatchView upd_view(Group& g, int cfg, cudaStream_t s) { return g.view(WORK_HALF,
 void launch_update(Group& g, int mode, int cfg, const BatchView& v, int par, int mu, unsigned hb_offset,
                    const InjView& inj, cudaStream_t s, int pdl = 0)
 {
-    if (cfg > 0) OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, cfg, par, mu, hb_offset, inj, pdl, s);
+    if (cfg == kCfgTile) OPS_CALL(g.N, update_tile, g.fp64, g.layout, mode, v, par, mu, hb_offset, inj, pdl, s);
+    else if (cfg > 0) OPS_CALL(g.N, update, g.fp64, g.layout, mode, v, cfg, par, mu, hb_offset, inj, pdl, s);
     else OPS_CALL(g.N, update_rows, g.fp64, g.layout, mode, v, -cfg, par, mu, hb_offset, inj, pdl, s);
 }
 
@@ -291,12 +308,17 @@ int update_block(sun_ctx* c, Group& g, int mode, cudaStream_t s)
         work += l->desc.halfV;
         bytes += l->bytes;
     }
+    // by size: SU(6) always tiled (1.6-2x faster than one thread per site
+    // from 12^4 up, no spills); small lattices of SU(4) and of SU(3) with
+    // FP64 full links row-split; everything else one thread per half-site
+    const bool small = work <= (g.fp64 ? c->rows_max_halfv / 2 : c->rows_max_halfv);
     const int fixed = c->upd_kernel == 1   ? c->blk_update
                       : c->upd_kernel == 2 ? -c->blk_rows
-                      : (work <= (g.fp64 ? c->rows_max_halfv / 2 : c->rows_max_halfv) &&
-                                 (g.N >= 4 || (g.N == 3 && g.fp64 && g.layout == SUN_SOA))
-                             ? -c->blk_rows
-                             : c->blk_update);
+                      : (c->upd_kernel == 3 && tile_ok(g)) ? kCfgTile
+                      : (g.N == 6 && tile_ok(g))             ? kCfgTile
+                      : (small && (g.N >= 4 || (g.N == 3 && g.fp64 && g.layout == SUN_SOA)))
+                          ? -c->blk_rows
+                          : c->blk_update;
     if (!c->tune) return fixed;
     char key[160];
     snprintf(key, sizeof key, "k_update N=%d %s layout=%d mode=%d halfV=%lld kernel=%d", g.N, g.fp64 ? "f64" : "f32",
@@ -318,8 +340,10 @@ int update_block(sun_ctx* c, Group& g, int mode, cudaStream_t s)
     InjView none{nullptr, 0, nullptr};
     int best = fixed;
     float best_ms = 1e30f;
-    for (int blk : {32, 64, 96, 128, -32, -64, -128}) {
-        if ((blk > 0 && c->upd_kernel == 2) || (blk < 0 && c->upd_kernel == 1)) continue;
+    for (int blk : {32, 64, 96, 128, -32, -64, -128, kCfgTile}) {
+        if (blk == kCfgTile && !tile_ok(g)) continue;
+        if (c->upd_kernel != 0 && (blk == kCfgTile) != (c->upd_kernel == 3)) continue;
+        if (blk != kCfgTile && ((blk > 0 && c->upd_kernel == 2) || (blk < 0 && c->upd_kernel == 1))) continue;
         BatchView v = upd_view(g, blk, s);
         launch_update(g, mode, blk, v, 0, 0, 0u, none, s);  // warm-up
         ck(cudaEventRecord(e0, s), "event");
@@ -441,7 +465,7 @@ void group_plaquette(sun_ctx* c, Group& g, double* out, cudaStream_t s)
 {
     double* r = group_reduce_fused(g, WORK_PLANES, c->blk_sites, 2, s,
                                    [&](const BatchView& v, double* part, double* out, unsigned* cnt) {
-                                       OPS_CALL(g.N, plaquette, g.fp64, g.layout, v, c->blk_sites, part, out, cnt, s);
+                                       OPS_CALL(g.N, plaquette, g.fp64, g.layout, v, c->blk_sites, part, out, cnt, nullptr, s);
                                    });
     for (size_t i = 0; i < g.lats.size(); ++i) {
         const LatDev& L = g.lats[i]->desc;
@@ -455,7 +479,7 @@ void group_polyakov(sun_ctx* c, Group& g, double* out, cudaStream_t s)
 {
     double* r = group_reduce_fused(g, WORK_POLY8, c->blk_sites, 2, s,
                                    [&](const BatchView& v, double* part, double* out, unsigned* cnt) {
-                                       OPS_CALL(g.N, polyakov, g.fp64, g.layout, v, c->blk_sites, part, out, cnt, s);
+                                       OPS_CALL(g.N, polyakov, g.fp64, g.layout, v, c->blk_sites, part, out, cnt, nullptr, s);
                                    });
     for (size_t i = 0; i < g.lats.size(); ++i) {
         const LatDev& L = g.lats[i]->desc;
@@ -489,6 +513,7 @@ struct Solo {
 sun_lattice::~sun_lattice()
 {
     if (sweep_graph) cudaGraphExecDestroy(sweep_graph);
+    if (meas_graph) cudaGraphExecDestroy(meas_graph);
     delete solo;
 }
 
@@ -559,8 +584,14 @@ __global__ void k_end_sweep(const LatDev* lats, int nlat, unsigned n_hb, unsigne
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nlat) {
-        lats[i].state[0] += n_hb;
-        lats[i].state[1] += inc;
+        unsigned* st = lats[i].state;
+        const unsigned lim = lats[i].sweep_limit;
+        const unsigned adv = lim == 0u || st[1] < lim;
+        if (adv) {
+            st[0] += n_hb;
+            st[1] += inc;
+        }
+        st[2] = adv;
     }
 }
 
@@ -574,6 +605,14 @@ cudaError_t launch_finalize_max(const BatchView& bv, const double* partials, dou
     k_finalize_max<<<bv.nlat, 32, 0, s>>>(bv, partials, out);
     return cudaGetLastError();
 }
+__global__ void k_bump(unsigned* slot) { *slot += 1u; }
+
+cudaError_t launch_bump(unsigned* slot, cudaStream_t s)
+{
+    k_bump<<<1, 1, 0, s>>>(slot);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_end_sweep(const LatDev* lats, int nlat, unsigned n_hb, unsigned inc, cudaStream_t s)
 {
     k_end_sweep<<<(nlat + 127) / 128, 128, 0, s>>>(lats, nlat, n_hb, inc);
@@ -670,9 +709,10 @@ sun_status sun_init(const sun_config* cfg, sun_ctx** out)
                     if (!c1) continue;
                     *c1 = 0;
                     int blk = atoi(c1 + 1);
-                    // k_update CTA sizes, or k_update_rows ones as negative numbers
+                    // k_update CTA sizes, k_update_rows ones as negative
+                    // numbers, or the tiled kernel's code
                     const int t = blk < 0 ? -blk : blk;
-                    if (t >= 32 && t <= 128 && t % 32 == 0) c->tuned[line] = blk;
+                    if ((t >= 32 && t <= 128 && t % 32 == 0) || blk == kCfgTile) c->tuned[line] = blk;
                 }
                 fclose(f);
             }
@@ -700,11 +740,13 @@ sun_status sun_init(const sun_config* cfg, sun_ctx** out)
         env_blk("SUN_B200_BLOCK_LINKS", c->blk_links);
         env_blk("SUN_B200_BLOCK_ROWS", c->blk_rows);
         if (c->blk_rows > 128) c->blk_rows = 128;
-        // update kernel: "sites" (k_update), "rows" (k_update_rows) or
-        // "auto" (by size); SUN_B200_ROWS_MAX_HALFV moves the size threshold
+        // update kernel: "sites" (k_update), "rows" (k_update_rows), "tile"
+        // (k_update_tile, N >= 4 full links; others by size) or "auto" (by
+        // size); SUN_B200_ROWS_MAX_HALFV moves the size threshold
         if (const char* k = getenv("SUN_B200_UPDATE_KERNEL")) {
             if (!strcmp(k, "sites")) c->upd_kernel = 1;
             else if (!strcmp(k, "rows")) c->upd_kernel = 2;
+            else if (!strcmp(k, "tile")) c->upd_kernel = 3;
         }
         if (const char* t = getenv("SUN_B200_ROWS_MAX_HALFV")) c->rows_max_halfv = atoll(t);
         if (const char* t = getenv("SUN_B200_PDL")) c->pdl = atoi(t) ? 1 : 0;
@@ -734,8 +776,8 @@ sun_status sun_lattice_create(sun_ctx* c, const sun_lattice_params* p, sun_latti
         const size_t csz = p->precision == SUN_F64 ? 16 : 8;
         l->bytes = csz * (size_t)elems_of(p->ncolors, p->layout) * 4 * (size_t)V;
         l->links.ensure(l->bytes);
-        l->state.ensure(2 * sizeof(unsigned));
-        ck(cudaMemset(l->state.p, 0, 2 * sizeof(unsigned)), "memset");
+        l->state.ensure(4 * sizeof(unsigned));
+        ck(cudaMemset(l->state.p, 0, 4 * sizeof(unsigned)), "memset");
         ck(cudaMemset(l->links.p, 0, l->bytes), "memset");
         LatDev& d = l->desc;
         d.links = l->links.p;
@@ -782,7 +824,7 @@ sun_status sun_lattice_init_cold(sun_lattice* l, void* stream)
         Solo so(l);
         BatchView v = so.g.view(WORK_LINKS, l->ctx->blk_links, s);
         OPS_CALL(l->p.ncolors, cold, so.g.fp64, so.g.layout, v, l->ctx->blk_links, s);
-        ck(cudaMemsetAsync(l->state.p, 0, 2 * sizeof(unsigned), s), "memset");
+        ck(cudaMemsetAsync(l->state.p, 0, 4 * sizeof(unsigned), s), "memset");
         ck(cudaStreamSynchronize(s), "cold start");
     });
 }
@@ -795,7 +837,7 @@ sun_status sun_lattice_init_hot(sun_lattice* l, void* stream)
         Solo so(l);
         BatchView v = so.g.view(WORK_SITES, 128, s);
         OPS_CALL(l->p.ncolors, hot, so.g.fp64, so.g.layout, v, 128, s);
-        ck(cudaMemsetAsync(l->state.p, 0, 2 * sizeof(unsigned), s), "memset");
+        ck(cudaMemsetAsync(l->state.p, 0, 4 * sizeof(unsigned), s), "memset");
         ck(cudaStreamSynchronize(s), "hot start");
     });
 }
@@ -914,6 +956,24 @@ sun_status sun_lattice_copy(sun_lattice* dst, sun_lattice* src, void* stream)
     return handle(dst->ctx, [&] { copy_links(dst, src, S(dst->ctx, stream)); });
 }
 
+sun_status sun_lattice_set_sweep_limit(sun_lattice* l, uint32_t limit)
+{
+    if (!l) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        if (l->desc.sweep_limit != limit) {
+            l->desc.sweep_limit = limit;
+            ++l->version;  // device tables and captured sweeps pick it up
+        }
+    });
+}
+
+sun_status sun_ctx_hbm_budget(const sun_ctx* c, size_t* bytes)
+{
+    if (!c || !bytes) return SUN_ERR_INVALID_ARG;
+    *bytes = c->hbm_budget;
+    return SUN_OK;
+}
+
 sun_status sun_lattice_get_rng(sun_lattice* l, uint64_t* seed, uint32_t* hb, uint32_t* sw)
 {
     if (!l) return SUN_ERR_INVALID_ARG;
@@ -1008,6 +1068,106 @@ sun_status sun_sweep(sun_lattice* l, int n_hb, int n_or, int n_sweeps, void* str
 {
     if (!l || n_hb < 0 || n_or < 0 || n_sweeps < 0) return SUN_ERR_INVALID_ARG;
     return handle(l->ctx, [&] { solo_passes(l, n_hb, n_or, n_sweeps, true, S(l->ctx, stream)); });
+}
+
+// The graph of sun_sweep_measure for at least `rows` sweeps (captured again
+// when the passes per sweep, the lattice descriptor or the row capacity
+// change).  Returns false when the caller's stream is being captured.
+static bool solo_measure_graph(sun_lattice* l, Group& g, int n_hb, int n_or, size_t rows, cudaStream_t s)
+{
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return false;
+    if (l->meas_graph && l->meas_hb == n_hb && l->meas_or == n_or && l->meas_version == l->version &&
+        l->meas_rows >= rows)
+        return true;
+    if (l->meas_graph) cudaGraphExecDestroy(l->meas_graph);
+    l->meas_graph = nullptr;
+    size_t cap_rows = 64;
+    while (cap_rows < rows) cap_rows *= 2;
+    l->meas.ensure(sizeof(double) * 4 * cap_rows);
+    l->slot.ensure(sizeof(unsigned));
+    l->meas_rows = cap_rows;
+    sun_ctx* c = l->ctx;
+    const bool re = l->p.reunit_every > 0;
+    // launch shapes, tables and scratch before the capture
+    if (n_hb > 0) upd_view(g, update_block(c, g, MODE_HB, s), s);
+    if (n_or > 0) upd_view(g, update_block(c, g, MODE_OR, s), s);
+    if (re) g.view(WORK_LINKS, c->blk_links, s);
+    BatchView vp = g.view(WORK_PLANES, c->blk_sites, s), vl = g.view(WORK_POLY8, c->blk_sites, s);
+    g.partials.ensure(sizeof(double) * 4 * (size_t)std::max(1, std::max(vp.nblocks, vl.nblocks)));
+    if (g.counters_n < g.lats.size()) {
+        g.counters.ensure(sizeof(unsigned) * g.lats.size());
+        ck(cudaMemsetAsync(g.counters.p, 0, sizeof(unsigned) * g.lats.size(), s), "counters");
+        g.counters_n = g.lats.size();
+    }
+    ck(cudaStreamSynchronize(s), "measure graph setup");
+    double* part = reinterpret_cast<double*>(g.partials.p);
+    unsigned* cnt = reinterpret_cast<unsigned*>(g.counters.p);
+    unsigned* slot = reinterpret_cast<unsigned*>(l->slot.p);
+    double* out_p = reinterpret_cast<double*>(l->meas.p);
+    double* out_l = out_p + 2 * cap_rows;
+    cudaStream_t cs;
+    ck(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+    cudaGraph_t graph;
+    ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "capture");
+    try {
+        group_sweep(c, g, n_hb, n_or, true, re, cs);
+        OPS_CALL(g.N, plaquette, g.fp64, g.layout, vp, c->blk_sites, part, out_p, cnt, slot, cs);
+        OPS_CALL(g.N, polyakov, g.fp64, g.layout, vl, c->blk_sites, part, out_l, cnt, slot, cs);
+        ck(launch_bump(slot, cs), "bump");
+    } catch (...) {
+        cudaStreamEndCapture(cs, &graph);
+        cudaStreamDestroy(cs);
+        throw;
+    }
+    ck(cudaStreamEndCapture(cs, &graph), "capture end");
+    cudaStreamDestroy(cs);
+    cudaError_t e = cudaGraphInstantiate(&l->meas_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) l->meas_graph = nullptr;
+    ck(e, "graph instantiate");
+    l->meas_hb = n_hb;
+    l->meas_or = n_or;
+    l->meas_version = l->version;
+    return true;
+}
+
+sun_status sun_sweep_measure(sun_lattice* l, int n_hb, int n_or, int n_sweeps, double* plaq, double* poly,
+                             void* stream)
+{
+    if (!l || n_hb < 0 || n_or < 0 || n_sweeps < 0) return SUN_ERR_INVALID_ARG;
+    return handle(l->ctx, [&] {
+        need_eo(l, "the heatbath/overrelaxation update");
+        cudaStream_t s = S(l->ctx, stream);
+        if (n_sweeps == 0) return;
+        Solo so(l);
+        if (solo_measure_graph(l, so.g, n_hb, n_or, (size_t)n_sweeps, s)) {
+            // n replays back to back, one copy of the observables at the end;
+            // normalised on the host as sun_plaquette / sun_polyakov do
+            ck(cudaMemsetAsync(l->slot.p, 0, sizeof(unsigned), s), "slot");
+            for (int i = 0; i < n_sweeps; ++i) ck(cudaGraphLaunch(l->meas_graph, s), "graph launch");
+            std::vector<double> h(4 * (size_t)n_sweeps);
+            const double* d = reinterpret_cast<const double*>(l->meas.p);
+            ck(cudaMemcpyAsync(h.data(), d, sizeof(double) * 2 * n_sweeps, cudaMemcpyDeviceToHost, s), "copy");
+            ck(cudaMemcpyAsync(h.data() + 2 * n_sweeps, d + 2 * l->meas_rows, sizeof(double) * 2 * n_sweeps,
+                               cudaMemcpyDeviceToHost, s),
+               "copy");
+            ck(cudaStreamSynchronize(s), "sweep and measure");
+            const LatDev& L = l->desc;
+            const double np = 3.0 * l->p.ncolors * (double)L.V, nl = (double)l->p.ncolors * L.X[0] * L.X[1] * L.X[2];
+            for (int i = 0; i < 2 * n_sweeps; ++i) {
+                if (plaq) plaq[i] = h[i] / np;
+                if (poly) poly[i] = h[2 * n_sweeps + i] / nl;
+            }
+            return;
+        }
+        double tmp[2];
+        for (int i = 0; i < n_sweeps; ++i) {
+            solo_passes(l, n_hb, n_or, 1, true, s);
+            group_plaquette(l->ctx, so.g, plaq ? plaq + 2 * i : tmp, s);
+            group_polyakov(l->ctx, so.g, poly ? poly + 2 * i : tmp, s);
+        }
+    });
 }
 
 sun_status sun_heatbath_injected(sun_lattice* l, const double* u, int stride, void* stream)
@@ -1304,8 +1464,31 @@ struct sun_batch {
     cudaGraphExec_t graph = nullptr;
     int graph_hb = -1, graph_or = -1;
     bool dirty = true;
+    // one stream and join event per class: in a captured sweep the classes
+    // are parallel branches
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> joined;
+    cudaEvent_t forked = nullptr;
 
-    ~sun_batch() { drop_graph(); }
+    ~sun_batch()
+    {
+        drop_graph();
+        for (auto st : branch) cudaStreamDestroy(st);
+        for (auto e : joined) cudaEventDestroy(e);
+        if (forked) cudaEventDestroy(forked);
+    }
+    void ensure_branches(size_t n)
+    {
+        if (!forked) ck(cudaEventCreateWithFlags(&forked, cudaEventDisableTiming), "event");
+        while (branch.size() < n) {
+            cudaStream_t st;
+            ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+            branch.push_back(st);
+            cudaEvent_t e;
+            ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+            joined.push_back(e);
+        }
+    }
     void drop_graph()
     {
         if (graph) cudaGraphExecDestroy(graph);
@@ -1342,9 +1525,26 @@ struct sun_batch {
 
 namespace {
 
-void batch_one_sweep(sun_batch* b, int n_hb, int n_or, cudaStream_t s)
+// One sweep of every class of the batch.  branches: each class on its own
+// stream, forked from s and joined back into it (inside a capture: parallel
+// branches of the graph, so the classes' launches overlap on the GPU).
+void batch_one_sweep(sun_batch* b, int n_hb, int n_or, cudaStream_t s, bool branches = false)
 {
-    for (auto& g : b->groups) group_sweep(b->ctx, *g, n_hb, n_or, true, group_needs_reunit(*g), s);
+    std::vector<Group*> act;
+    for (auto& g : b->groups)
+        if (!g->lats.empty()) act.push_back(g.get());
+    if (!branches || act.size() < 2) {
+        for (auto* g : act) group_sweep(b->ctx, *g, n_hb, n_or, true, group_needs_reunit(*g), s);
+        return;
+    }
+    b->ensure_branches(act.size());
+    ck(cudaEventRecord(b->forked, s), "fork");
+    for (size_t i = 0; i < act.size(); ++i) {
+        ck(cudaStreamWaitEvent(b->branch[i], b->forked, 0), "fork");
+        group_sweep(b->ctx, *act[i], n_hb, n_or, true, group_needs_reunit(*act[i]), b->branch[i]);
+        ck(cudaEventRecord(b->joined[i], b->branch[i]), "join");
+    }
+    for (size_t i = 0; i < act.size(); ++i) ck(cudaStreamWaitEvent(s, b->joined[i], 0), "join");
 }
 
 }  // namespace
@@ -1424,8 +1624,9 @@ sun_status sun_batch_sweep(sun_batch* b, int n_hb, int n_or, int n_sweeps, int u
             ck(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
             cudaGraph_t graph;
             ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "capture");
+            b->ensure_branches(b->groups.size());  // streams and events exist before the capture
             try {
-                batch_one_sweep(b, n_hb, n_or, cs);
+                batch_one_sweep(b, n_hb, n_or, cs, true);
             } catch (...) {
                 cudaStreamEndCapture(cs, &graph);
                 cudaStreamDestroy(cs);
@@ -1465,6 +1666,34 @@ static sun_status batch_measure(sun_batch* b, double* out, void* stream, bool pl
 }
 
 sun_status sun_batch_plaquette(sun_batch* b, double* out, void* stream) { return batch_measure(b, out, stream, true); }
+
+sun_status sun_batch_wilson_loops(sun_batch* b, int R, int T, double* out, void* stream)
+{
+    if (!b || !out) return SUN_ERR_INVALID_ARG;
+    return handle(b->ctx, [&] {
+        if (R < 0 || T < 0 || R > 8 || T > 8) fail(SUN_ERR_INVALID_ARG, "Wilson loops need 0 <= R, T <= 8");
+        for (auto* l : b->order) {
+            for (int d = 0; d < 3; ++d)
+                if (R >= l->p.dims[d]) fail(SUN_ERR_INVALID_ARG, "R=%d not below spatial extent %d", R, l->p.dims[d]);
+            if (T >= l->p.dims[3]) fail(SUN_ERR_INVALID_ARG, "T=%d not below temporal extent", T);
+        }
+        b->regroup();
+        cudaStream_t s = S(b->ctx, stream);
+        const int nv = 2 * (R + 1) * (T + 1);
+        const int blk = b->ctx->blk_wilson;
+        for (auto& g : b->groups) {
+            if (g->lats.empty()) continue;
+            double* r = group_reduce(*g, WORK_SITES, blk, nv, false, s, [&](const BatchView& v, double* part) {
+                OPS_CALL(g->N, wilson, g->fp64, g->layout, v, blk, R, T, part, s);
+            });
+            for (size_t i = 0; i < g->lats.size(); ++i) {
+                const size_t pos = std::find(b->order.begin(), b->order.end(), g->lats[i]) - b->order.begin();
+                const double norm = 3.0 * g->N * (double)g->lats[i]->desc.V;
+                for (int k = 0; k < nv; ++k) out[pos * nv + k] = r[i * nv + k] / norm;
+            }
+        }
+    });
+}
 sun_status sun_batch_polyakov(sun_batch* b, double* out, void* stream) { return batch_measure(b, out, stream, false); }
 
 }  // extern "C"

@@ -37,7 +37,10 @@ static __device__ __align__(256) double g_plaq_scratch[4 * kMaxBlocks];
 
 // Host code cannot use g_plaq_scratch's name as a device address (it names a
 // host-side stand-in).  The device address is looked up once per device,
-// with that device current, and cached here.
+// with that device current, and cached here for the life of the process: a
+// caller that destroys and re-creates a device's context (cudaDeviceReset)
+// must not call this entry point afterwards, since the cached address
+// belonged to the old context.
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 double* g_scratch_addr[kMaxDevices] = {};
@@ -139,17 +142,27 @@ extern "C" sun_status sun_plaquette_noalloc(const void* d_links, const sun_latti
         return reject(SUN_ERR_UNSUPPORTED, "sun_plaquette_noalloc: 12/8-parameter layouts are SU(3) only");
     if (p->layout != SUN_SOA && p->layout != SUN_SOA12 && p->layout != SUN_SOA8)
         return reject(SUN_ERR_INVALID_ARG, "sun_plaquette_noalloc: unknown layout");
+    if (p->precision != SUN_F32 && p->precision != SUN_F64)
+        return reject(SUN_ERR_INVALID_ARG, "sun_plaquette_noalloc: unknown precision");
+    if (p->order != SUN_EVEN_ODD && p->order != SUN_NORMAL)
+        return reject(SUN_ERR_INVALID_ARG, "sun_plaquette_noalloc: unknown storage order");
+    // the site count, checked against the scratch limit before every
+    // multiplication (no overflow whatever the dimensions)
     long long V = 1;
     for (int d = 0; d < 4; ++d) {
         if (p->dims[d] < 2 || p->dims[d] % 2)
             return reject(SUN_ERR_INVALID_ARG, "sun_plaquette_noalloc: every dimension must be even and >= 2");
+        if (p->dims[d] > kMaxSites || V > kMaxSites) {
+            V = kMaxSites + 1;
+            break;
+        }
         V *= p->dims[d];
     }
     if (V > kMaxSites) {
         char msg[200];
         snprintf(msg, sizeof msg,
-                 "sun_plaquette_noalloc: %lld sites exceed the fixed scratch (at most %lld sites); "
-                 "use sun_plaquette", V, kMaxSites);
+                 "sun_plaquette_noalloc: the lattice's sites exceed the fixed scratch (at most %lld sites); "
+                 "use sun_plaquette", kMaxSites);
         return reject(SUN_ERR_CAPACITY, msg);
     }
     int dev = 0;

@@ -2,15 +2,21 @@
 //
 // A job is (N, L^3 x T, beta, sweeps, observables).  Jobs queue FIFO; each
 // scheduling step admits queued jobs while a slot is free and their HBM
-// footprint fits the budget, advances every active job by one sweep -- all
-// active lattices of one (n_hb, n_or) kind in one batched launch per phase --
-// then measures and retires the jobs that finished.  Links and RNG counters
+// footprint fits the budget, advances every active job by up to K sweeps --
+// all active lattices of one (n_hb, n_or) kind replayed from one captured
+// graph, the (N, precision, layout) classes as parallel branches of it --
+// then measures the jobs that finished in one batched launch per class and
+// observable and retires them.  Each job's lattice carries its sweep count as
+// a device-side limit, so a job that finishes inside a step sits out the
+// rest of it unchanged: K only sets how often the host admits and retires
+// (K is chosen so a step lasts about step_target_s).  Links and RNG counters
 // stay on the device for a job's whole life.  Because the random stream of a
 // link is keyed only by (seed, site, direction, heatbath pass) and the
 // reductions are per-lattice and fixed-order, a job's result does not depend
 // on which other jobs shared its launches.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <deque>
@@ -90,14 +96,19 @@ struct sun_server {
     std::deque<Pending> queue;
     std::vector<Active> active;
     std::map<std::pair<int, int>, sun_batch*> batches;
+    sun_batch* retiring = nullptr;  // the jobs measured together at a step's end
     std::deque<sun_result> outbox;  // finished results not yet returned
     int64_t next_id = 1;
     double t0 = 0;
+    // sweeps per step: about step_target_s of GPU work, at most k_max
+    double step_target_s = 0.05, sweep_s = 0.0;
+    int k_max = 16;
 
     ~sun_server()
     {
         for (auto& a : active) sun_lattice_destroy(a.lat);
         for (auto& kv : batches) sun_batch_destroy(kv.second);
+        if (retiring) sun_batch_destroy(retiring);
     }
     double now() const { return clock_s() - t0; }
     sun_batch* batch_for(const sun_job& j)
@@ -143,12 +154,12 @@ sun_status sun_server_create(sun_ctx* ctx, int max_active, sun_server** out)
     sun_server* s = new sun_server();
     s->ctx = ctx;
     s->max_active = max_active;
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    // the context's admission budget (sun_config.hbm_budget_bytes, or 90 %
+    // of the free memory at sun_init)
+    if (sun_ctx_hbm_budget(ctx, &s->budget) != SUN_OK || sun_batch_create(ctx, &s->retiring) != SUN_OK) {
         delete s;
-        return SUN_ERR_CUDA;
+        return SUN_ERR_INVALID_ARG;
     }
-    s->budget = (size_t)(0.85 * (double)fr);
     s->t0 = clock_s();
     *out = s;
     return SUN_OK;
@@ -228,6 +239,7 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
             if (st == SUN_ERR_OUT_OF_MEMORY) break;  // retry at the next step
             s->queue.pop_front();
             if (st == SUN_OK) st = j.hot_start ? sun_lattice_init_hot(lat, nullptr) : sun_lattice_init_cold(lat, nullptr);
+            if (st == SUN_OK) st = sun_lattice_set_sweep_limit(lat, (uint32_t)j.sweeps);
             sun_batch* b = (st == SUN_OK && j.sweeps > 0) ? s->batch_for(j) : nullptr;
             if (st == SUN_OK && j.sweeps > 0 && !b) st = SUN_ERR_CUDA;
             if (st == SUN_OK && b) st = sun_batch_add(b, lat);
@@ -248,37 +260,78 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
             s->active.push_back(a);
         }
     }
-    // 2. one sweep of every active job, batched per (n_hb, n_or)
-    for (auto& kv : s->batches) {
-        int n = 0;
-        sun_batch_size(kv.second, &n);
-        if (n == 0) continue;
-        // only lattices with sweeps left are in a batch
-        sun_status st = sun_batch_sweep(kv.second, kv.first.first, kv.first.second, 1, 0, nullptr);
-        if (st != SUN_OK) return st;
-    }
-    // 3. retire
-    std::vector<sun_server::Active> keep;
-    for (auto& a : s->active) {
-        if (a.remaining > 0) --a.remaining;
-        if (a.remaining > 0) {
-            keep.push_back(a);
-            continue;
+    // 2. up to K sweeps of every active job, batched per (n_hb, n_or); a job
+    // with fewer sweeps left stops at its own count (device-side limit)
+    int left_max = 0;
+    for (auto& a : s->active) left_max = std::max(left_max, a.remaining);
+    if (left_max > 0) {
+        int k = s->sweep_s > 0 ? (int)(s->step_target_s / s->sweep_s + 0.5) : 1;
+        k = std::max(1, std::min(std::min(k, s->k_max), left_max));
+        const double ts = clock_s();
+        for (auto& kv : s->batches) {
+            int n = 0;
+            sun_batch_size(kv.second, &n);
+            if (n == 0) continue;
+            sun_status st = sun_batch_sweep(kv.second, kv.first.first, kv.first.second, k, 1, nullptr);
+            if (st != SUN_OK) return st;
         }
-        sun_result r = blank_result(a.id, SUN_OK, a.submit_s);
-        r.start_s = a.start_s;
-        sun_status st = SUN_OK;
-        if (a.job.observables & 1) st = sun_plaquette(a.lat, r.plaquette, nullptr);
-        if (st == SUN_OK && (a.job.observables & 2)) st = sun_polyakov(a.lat, r.polyakov, nullptr);
-        if (st == SUN_OK && (a.job.observables & 4)) st = sun_wilson_loops(a.lat, a.job.wilson_R, a.job.wilson_T, r.wilson, nullptr);
-        r.status = st;
-        r.finish_s = s->now();
-        const double V = (double)a.job.dims[0] * a.job.dims[1] * a.job.dims[2] * a.job.dims[3];
-        r.link_updates = (double)a.job.sweeps * (a.job.n_hb + a.job.n_or) * 4.0 * V;
-        if (a.job.sweeps > 0) sun_batch_remove(s->batch_for(a.job), a.lat);
-        sun_lattice_destroy(a.lat);
-        s->used -= a.bytes;
-        emit(r);
+        const double per = (clock_s() - ts) / k;
+        s->sweep_s = s->sweep_s > 0 ? 0.5 * (s->sweep_s + per) : per;
+        for (auto& a : s->active) a.remaining = std::max(0, a.remaining - k);
+    }
+    // 3. measure the finished jobs together (one launch per class and
+    // observable), then retire them
+    std::vector<sun_server::Active> keep, fin;
+    for (auto& a : s->active) (a.remaining > 0 ? keep : fin).push_back(a);
+    if (!fin.empty()) {
+        std::vector<sun_result> res(fin.size());
+        std::vector<sun_status> stat(fin.size(), SUN_OK);
+        for (size_t i = 0; i < fin.size(); ++i) {
+            res[i] = blank_result(fin[i].id, SUN_OK, fin[i].submit_s);
+            res[i].start_s = fin[i].start_s;
+        }
+        auto measure = [&](int bit, int R, int T) {
+            std::vector<size_t> idx;
+            for (size_t i = 0; i < fin.size(); ++i)
+                if ((fin[i].job.observables & bit) && stat[i] == SUN_OK &&
+                    (bit != 4 || (fin[i].job.wilson_R == R && fin[i].job.wilson_T == T)))
+                    idx.push_back(i);
+            if (idx.empty()) return;
+            for (size_t i : idx) sun_batch_add(s->retiring, fin[i].lat);
+            const int nv = bit == 4 ? 2 * (R + 1) * (T + 1) : 2;
+            std::vector<double> out(nv * idx.size());
+            sun_status st = bit == 1   ? sun_batch_plaquette(s->retiring, out.data(), nullptr)
+                            : bit == 2 ? sun_batch_polyakov(s->retiring, out.data(), nullptr)
+                                       : sun_batch_wilson_loops(s->retiring, R, T, out.data(), nullptr);
+            for (size_t q = 0; q < idx.size(); ++q) {
+                const size_t i = idx[q];
+                if (st != SUN_OK) stat[i] = st;
+                else if (bit == 1) memcpy(res[i].plaquette, &out[2 * q], 2 * sizeof(double));
+                else if (bit == 2) memcpy(res[i].polyakov, &out[2 * q], 2 * sizeof(double));
+                else memcpy(res[i].wilson, &out[nv * q], nv * sizeof(double));
+                sun_batch_remove(s->retiring, fin[i].lat);
+            }
+        };
+        measure(1, 0, 0);
+        measure(2, 0, 0);
+        std::vector<std::pair<int, int>> rts;
+        for (auto& a : fin)
+            if ((a.job.observables & 4) &&
+                std::find(rts.begin(), rts.end(), std::make_pair(a.job.wilson_R, a.job.wilson_T)) == rts.end())
+                rts.emplace_back(a.job.wilson_R, a.job.wilson_T);
+        for (auto& rt : rts) measure(4, rt.first, rt.second);
+        for (size_t i = 0; i < fin.size(); ++i) {
+            sun_server::Active& a = fin[i];
+            sun_result& r = res[i];
+            r.status = stat[i];
+            r.finish_s = s->now();
+            const double V = (double)a.job.dims[0] * a.job.dims[1] * a.job.dims[2] * a.job.dims[3];
+            r.link_updates = (double)a.job.sweeps * (a.job.n_hb + a.job.n_or) * 4.0 * V;
+            if (a.job.sweeps > 0) sun_batch_remove(s->batch_for(a.job), a.lat);
+            sun_lattice_destroy(a.lat);
+            s->used -= a.bytes;
+            emit(r);
+        }
     }
     s->active.swap(keep);
     int done = 0;

@@ -125,8 +125,8 @@ template <class R, class Stream> SUN_DEV void su2_heatbath_draw(R al, Stream& st
     R xr2 = M::log_(st.uniform() + tiny);
     R xr3 = M::cos2pi(st.uniform());
     R xr4 = st.uniform();
-    R d = -(xr2 + xr1 * xr3 * xr3) / al;
-    bool accepted = (R(1) - R(0.5) * d) > xr4 * xr4;
+    R d = -fma(xr1 * xr3, xr3, xr2) / al;
+    bool accepted = fma(R(-0.5), d, R(1)) > xr4 * xr4;
     if (!accepted) {
         if (al > R(2)) {
             for (int k = 0; k < 20; ++k) {
@@ -134,8 +134,8 @@ template <class R, class Stream> SUN_DEV void su2_heatbath_draw(R al, Stream& st
                 xr2 = M::log_(st.uniform() + tiny);
                 xr3 = M::cos2pi(st.uniform());
                 xr4 = st.uniform();
-                d = -(xr2 + xr1 * xr3 * xr3) / al;
-                if ((R(1) - R(0.5) * d) > xr4 * xr4) break;
+                d = -fma(xr1 * xr3, xr3, xr2) / al;
+                if (fma(R(-0.5), d, R(1)) > xr4 * xr4) break;
             }
         } else {
             const R e = M::exp_(R(-2) * al);
@@ -144,21 +144,44 @@ template <class R, class Stream> SUN_DEV void su2_heatbath_draw(R al, Stream& st
             for (int k = 0; k < 20; ++k) {
                 R u1 = st.uniform();
                 R u2 = st.uniform();
-                a0 = R(1) + M::log_(e + w * u1) / al;
-                if ((R(1) - a0 * a0) > u2 * u2) break;
+                a0 = R(1) + M::log_(fma(w, u1, e)) / al;
+                if (fma(-a0, a0, R(1)) > u2 * u2) break;
             }
             d = R(1) - a0;
         }
     }
     R a0 = R(1) - d;
-    R rr = fabs(R(1) - a0 * a0);
+    R rr = fabs(fma(-a0, a0, R(1)));
     a[0] = a0;
-    a[3] = (R(2) * st.uniform() - R(1)) * M::sqrt_(rr);
-    R x1 = M::sqrt_(fabs(rr - a[3] * a[3]));
+    a[3] = fma(R(2), st.uniform(), R(-1)) * M::sqrt_(rr);
+    R x1 = M::sqrt_(fabs(fma(-a[3], a[3], rr)));
     R s, c;
     M::sincos2pi(st.uniform(), &s, &c);
     a[1] = x1 * c;
     a[2] = x1 * s;
+}
+
+// Arithmetic of the SU(2) draw in FP32 updates (SUN_F32_DRAW): 0 FP32 with
+// the hardware log / exp / sincos approximations; 1 FP64 arithmetic on the
+// same 24-bit uniforms (the accept/reject tests then see only the FP32
+// rounding of alpha, not that of the transcendentals).
+#ifndef SUN_F32_DRAW
+#define SUN_F32_DRAW 0
+#endif
+template <class Stream> struct WideStream {
+    Stream& s;
+    SUN_DEV double uniform() { return (double)s.uniform(); }
+};
+template <class R, class Stream> SUN_DEV void su2_draw(R al, Stream& st, R a[4])
+{
+    if constexpr (sizeof(R) == 4 && SUN_F32_DRAW == 1) {
+        WideStream<Stream> w{st};
+        double ad[4];
+        su2_heatbath_draw<double>((double)al, w, ad);
+        a[0] = (R)ad[0]; a[1] = (R)ad[1]; a[2] = (R)ad[2]; a[3] = (R)ad[3];
+    } else {
+        su2_heatbath_draw<R>(al, st, a);
+    }
 }
 
 // Cabibbo-Marinari pseudo-heatbath of U against the staple sum S (F = S^dag)
@@ -179,11 +202,11 @@ SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, St
             if (b == 0) su2_block_US<N, R>(U, S, 0, 1, r);
             else if (b == 1) su2_block_US<N, R>(U, S, 1, 2, r);
             else su2_block_US<N, R>(U, S, 0, 2, r);
-            R k = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+            R k = sqrt(qnorm2(r));
             R ap = beta_over_n * k;
             k = R(1) / k;
             r[0] *= k; r[1] *= k; r[2] *= k; r[3] *= k;
-            su2_heatbath_draw<R>(ap, st, a);
+            su2_draw<R>(ap, st, a);
             su2_mul_udag(a, r, c);
             if (b == 0) su2_apply<N, R>(U, 0, 1, c);
             else if (b == 1) su2_apply<N, R>(U, 1, 2, c);
@@ -198,11 +221,11 @@ SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, St
         for (int b = 0; b < SubGroup<N>::count; ++b) {
             R r[4], a[4], c[4];
             with_subgroup<N>(b, [&](auto P, auto Q) { su2_block_US<N, R>(U, S, P(), Q(), r); });
-            R k = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+            R k = sqrt(qnorm2(r));
             R ap = beta_over_n * k;
             k = R(1) / k;
             r[0] *= k; r[1] *= k; r[2] *= k; r[3] *= k;
-            su2_heatbath_draw<R>(ap, st, a);
+            su2_draw<R>(ap, st, a);
             su2_mul_udag(a, r, c);
             with_subgroup<N>(b, [&](auto P, auto Q) { su2_apply<N, R>(U, P(), Q(), c); });
         }
@@ -214,11 +237,11 @@ SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, St
             const int p = SubGroup<N>::p(b), q = SubGroup<N>::q(b);
             R r[4], a[4], c[4];
             su2_block<N, R>(M, p, q, r);
-            R k = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+            R k = sqrt(qnorm2(r));
             R ap = beta_over_n * k;
             k = R(1) / k;
             r[0] *= k; r[1] *= k; r[2] *= k; r[3] *= k;
-            su2_heatbath_draw<R>(ap, st, a);
+            su2_draw<R>(ap, st, a);
             su2_mul_udag(a, r, c);
             su2_apply<N, R>(U, p, q, c);
             su2_apply<N, R>(M, p, q, c);
@@ -233,11 +256,11 @@ SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, St
 // same SU(2) element with half the row arithmetic.
 template <class R> SUN_DEV void su2_overrelax_element(const R r[4], R c[4])
 {
-    const R n2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3];
+    const R n2 = qnorm2(r);
     const R inv = R(1) / n2;
     // a = (r0, -r1, -r2, -r3)/|r|  ->  a^2 = ((r0^2 - |r_vec|^2), -2 r0 r_vec) / |r|^2
     const R t = R(-2) * r[0] * inv;
-    c[0] = (r[0] * r[0] - (r[1] * r[1] + r[2] * r[2] + r[3] * r[3])) * inv;
+    c[0] = fma(r[0], r[0], -fma(r[3], r[3], fma(r[2], r[2], r[1] * r[1]))) * inv;
     c[1] = t * r[1];
     c[2] = t * r[2];
     c[3] = t * r[3];
@@ -403,6 +426,47 @@ template <int N, class R, int LAYOUT> struct LinkIO {
             A.e[1][0] = ld_elem<R, NC>(base + idx + 2 * stride);
             cx<R> th = ld_elem<R, NC>(base + idx + 3 * stride);
             rebuild8<R>(A, th.re, th.im);
+        }
+    }
+    // the same loads and store through element accessors: f(idx, e) returns
+    // element e of the link at image index idx (complex element
+    // idx + e stride of the image), w(idx, e, v) writes it
+    template <class F> static SUN_DEV void load_rows_f(F&& f, uint32_t idx, uint32_t stride, Mat<N, R>& A)
+    {
+        static_assert(LAYOUT == L_SOA12, "stored rows exist for SOA12 only");
+#pragma unroll
+        for (int e = 0; e < 6; ++e) A.e[e / 3][e % 3] = f(idx, e);
+    }
+    template <class F> static SUN_DEV void load_f(F&& f, uint32_t idx, uint32_t stride, Mat<N, R>& A)
+    {
+        if constexpr (LAYOUT == L_SOA) {
+#pragma unroll
+            for (int e = 0; e < N * N; ++e) A.e[e / N][e % N] = f(idx, e);
+        } else if constexpr (LAYOUT == L_SOA12) {
+#pragma unroll
+            for (int e = 0; e < 6; ++e) A.e[e / 3][e % 3] = f(idx, e);
+            rebuild12<R>(A);
+        } else {
+            A.e[0][1] = f(idx, 0);
+            A.e[0][2] = f(idx, 1);
+            A.e[1][0] = f(idx, 2);
+            cx<R> th = f(idx, 3);
+            rebuild8<R>(A, th.re, th.im);
+        }
+    }
+    template <class W> static SUN_DEV void store_f(W&& w, uint32_t idx, uint32_t stride, const Mat<N, R>& A)
+    {
+        if constexpr (LAYOUT == L_SOA) {
+#pragma unroll
+            for (int e = 0; e < N * N; ++e) w(idx, e, A.e[e / N][e % N]);
+        } else if constexpr (LAYOUT == L_SOA12) {
+#pragma unroll
+            for (int e = 0; e < 6; ++e) w(idx, e, A.e[e / 3][e % 3]);
+        } else {
+            w(idx, 0, A.e[0][1]);
+            w(idx, 1, A.e[0][2]);
+            w(idx, 2, A.e[1][0]);
+            w(idx, 3, mkc<R>(atan2(A.e[0][0].im, A.e[0][0].re), atan2(A.e[2][0].im, A.e[2][0].re)));
         }
     }
     static SUN_DEV void store(cx<R>* base, uint32_t idx, uint32_t stride, const Mat<N, R>& A)

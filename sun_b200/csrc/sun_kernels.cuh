@@ -89,25 +89,16 @@ template <class R, int MODE, int LAYOUT> struct UpdateOccupancy<3, R, MODE, LAYO
 };
 
 // ---------------------------------------------------------------------------
-// Checkerboard update of the links (x, mu) with parity(x) == parity --
-// kernel_PHeatBath_evenodd (src/monte/monte.cu:44-88) and
-// kernel_overrelaxation_evenodd (src/monte/ovr.cu:41-80).  One thread per
-// half-lattice site; the staples are summed "up" then "down" per nu, nu in
-// the reference's ascending order for N = 6 and in the order mu+1, mu+2,
-// mu+3 (mod 4) for N <= 4 (see below); all links are read through L2 only
-// (LD_CG: the launch overlaps the previous phase's, see the pdl note below).
-template <int N, class R, int LAYOUT, int MODE>
-__global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE, LAYOUT>::min_blocks)) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
-                                                InjView inj, int pdl)
+// One link update of the checkerboard phase (parity, mu): half-site id of
+// lattice L.  ld(i, e) returns element e of the link at image index i
+// (complex element i + 4 V e) and st(i, e, v) writes it.  GDC: the launch
+// may be a programmatic dependent of the previous phase (pdl != 0 then waits
+// for it before the staples of the direction that phase wrote).
+template <int N, class R, int LAYOUT, int MODE, bool GDC, class Ld, class St>
+SUN_DEV void update_site(const Geom& g, const LatDev& L, int id, int parity, int mu, unsigned hb_offset,
+                         const InjView& inj, int pdl, Ld&& ld, St&& st)
 {
-    const int b = blockIdx.x;
-    const int l = find_lat(bv, b);
-    const LatDev& L = bv.lats[l];
-    const Geom g = geom_of(L);
-    const int id = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
-    if (id >= g.halfV) return;
     typedef LinkIO<N, R, LAYOUT> IO;
-    const cx<R>* base = reinterpret_cast<const cx<R>*>(L.links);
     const uint32_t V = (uint32_t)g.V, stride = 4u * V;
 
     int x[4];
@@ -116,11 +107,11 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE, LAYOUT>::min
     const int sx = id + parity * H;
     // neighbours by lexicographic stepping: lex +- stride_d with the periodic
     // wrap, then even/odd index (lex >> 1) + parity * V/2
-    const int st[4] = {1, g.X[0], g.X[0] * g.X[1], g.X[0] * g.X[1] * g.X[2]};
-    const int lex = x[0] + st[1] * x[1] + st[2] * x[2] + st[3] * x[3];
+    const int st_[4] = {1, g.X[0], g.X[0] * g.X[1], g.X[0] * g.X[1] * g.X[2]};
+    const int lex = x[0] + st_[1] * x[1] + st_[2] * x[2] + st_[3] * x[3];
     const int xm = mu == 0 ? x[0] : (mu == 1 ? x[1] : (mu == 2 ? x[2] : x[3]));
     const int Xm = mu == 0 ? g.X[0] : (mu == 1 ? g.X[1] : (mu == 2 ? g.X[2] : g.X[3]));
-    const int Sm = mu == 0 ? st[0] : (mu == 1 ? st[1] : (mu == 2 ? st[2] : st[3]));
+    const int Sm = mu == 0 ? st_[0] : (mu == 1 ? st_[1] : (mu == 2 ? st_[2] : st_[3]));
     const int other = (1 - parity) * H;
     const int sxpmu = (lex_step(lex, xm, Xm, Sm, 1) >> 1) + other;
 
@@ -130,8 +121,10 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE, LAYOUT>::min
     // the previous launch drains; griddepcontrol.wait then waits for it to
     // complete, and only after that the next phase may launch (so a launch
     // never runs beside the one two back).
-    const int dep = pdl ? ((mu + 3) & 3) : -1;
-    if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int dep = (GDC && pdl) ? ((mu + 3) & 3) : -1;
+    if constexpr (GDC) {
+        if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    }
     Mat<N, R> S;
     mzero(S);
     // N <= 4: nu = mu+1, mu+2, mu+3 (mod 4), the staple of the previous
@@ -143,12 +136,12 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE, LAYOUT>::min
     for (int kk = kRot ? 1 : 0; kk < 4; ++kk) {
         const int nu = kRot ? ((mu + kk) & 3) : kk;
         if (!kRot && nu == mu) continue;
-        if (nu == dep) {
+        if (GDC && nu == dep) {
             asm volatile("griddepcontrol.wait;" ::: "memory");
             asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
         }
         const int xn_ = kRot ? sel4(x, nu) : x[kk], Xn_ = kRot ? sel4(g.X, nu) : g.X[kk],
-                  Sn_ = kRot ? sel4(st, nu) : st[kk];
+                  Sn_ = kRot ? sel4(st_, nu) : st_[kk];
         const int lup = lex_step(lex, xn_, Xn_, Sn_, 1);
         const int ldn = lex_step(lex, xn_, Xn_, Sn_, -1);
         const int syp = (lup >> 1) + other;                               // x + nu
@@ -160,57 +153,81 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE, LAYOUT>::min
             // only its rows 0, 1 are multiplied out (from the stored rows of
             // the left factor, which is not rebuilt) and row 2 is rebuilt as
             // conj(row0 x row1) -- 36 fewer real FMAs per staple
-            IO::template load_rows<LD_CG>(base, sx + nu * V, stride, A);
-            IO::template load<LD_CG>(base, syp + mu * V, stride, B);
+            IO::load_rows_f(ld, sx + nu * V, stride, A);
+            IO::load_f(ld, syp + mu * V, stride, B);
             mmul_rows01(A, B, C);
             rebuild12(C);
-            IO::template load<LD_CG>(base, sxpmu + nu * V, stride, A);
+            IO::load_f(ld, sxpmu + nu * V, stride, A);
             macc_nd(C, A, S);
             // down: U_nu(x-nu)^dagger [U_mu(x-nu) U_nu(x-nu+mu)]
-            IO::template load_rows<LD_CG>(base, sy + mu * V, stride, A);
-            IO::template load<LD_CG>(base, sz + nu * V, stride, B);
+            IO::load_rows_f(ld, sy + mu * V, stride, A);
+            IO::load_f(ld, sz + nu * V, stride, B);
             mmul_rows01(A, B, C);
             rebuild12(C);
-            IO::template load<LD_CG>(base, sy + nu * V, stride, A);
+            IO::load_f(ld, sy + nu * V, stride, A);
             macc_dn(A, C, S);
         } else {
             // up: U_nu(x) U_mu(x+nu) U_nu(x+mu)^dagger
-            IO::template load<LD_CG>(base, sx + nu * V, stride, A);
-            IO::template load<LD_CG>(base, syp + mu * V, stride, B);
+            IO::load_f(ld, sx + nu * V, stride, A);
+            IO::load_f(ld, syp + mu * V, stride, B);
             mmul(A, B, C);
-            IO::template load<LD_CG>(base, sxpmu + nu * V, stride, A);
+            IO::load_f(ld, sxpmu + nu * V, stride, A);
             macc_nd(C, A, S);
             // down: U_nu(x-nu)^dagger U_mu(x-nu) U_nu(x-nu+mu)
-            IO::template load<LD_CG>(base, sy + nu * V, stride, A);
-            IO::template load<LD_CG>(base, sy + mu * V, stride, B);
+            IO::load_f(ld, sy + nu * V, stride, A);
+            IO::load_f(ld, sy + mu * V, stride, B);
             mmul_dn(A, B, C);
-            IO::template load<LD_CG>(base, sz + nu * V, stride, A);
+            IO::load_f(ld, sz + nu * V, stride, A);
             macc(C, A, S);
         }
     }
 
-    cx<R>* wbase = reinterpret_cast<cx<R>*>(L.links);
     const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
     Mat<N, R> U;
-    IO::template load<LD_CG>(wbase, own, stride, U);
+    IO::load_f(ld, own, stride, U);
     if constexpr (N == 3 && LAYOUT == L_SOA12) unit_row2<R>(U);
     if constexpr (MODE == MODE_OR) {
         overrelax_update<N, R>(U, S);
     } else {
         const R bon = (R)L.beta_over_n;
         if constexpr (MODE == MODE_HB) {
-            PhiloxStream<R> st;
-            st.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
-            heatbath_update<N, R>(U, S, bon, st);
+            PhiloxStream<R> ph;
+            ph.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
+            heatbath_update<N, R>(U, S, bon, ph);
         } else {
-            InjectedStream<R> st;
-            st.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
-            st.left = inj.stride;
-            st.err = inj.err;
-            heatbath_update<N, R>(U, S, bon, st);
+            InjectedStream<R> is;
+            is.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
+            is.left = inj.stride;
+            is.err = inj.err;
+            heatbath_update<N, R>(U, S, bon, is);
         }
     }
-    IO::store(wbase, own, stride, U);
+    IO::store_f(st, own, stride, U);
+}
+
+// Checkerboard update of the links (x, mu) with parity(x) == parity --
+// kernel_PHeatBath_evenodd (src/monte/monte.cu:44-88) and
+// kernel_overrelaxation_evenodd (src/monte/ovr.cu:41-80).  One thread per
+// half-lattice site; the staples are summed "up" then "down" per nu, nu in
+// the reference's ascending order for N = 6 and in the order mu+1, mu+2,
+// mu+3 (mod 4) for N <= 4 (see update_site); all links are read through L2
+// only (LD_CG: the launch overlaps the previous phase's).
+template <int N, class R, int LAYOUT, int MODE>
+__global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE, LAYOUT>::min_blocks)) k_update(BatchView bv, int parity, int mu, unsigned hb_offset,
+                                                InjView inj, int pdl)
+{
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int id = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    if (id >= g.halfV || lat_frozen(L)) return;
+    cx<R>* base = reinterpret_cast<cx<R>*>(L.links);
+    const uint32_t stride = 4u * (uint32_t)g.V;
+    update_site<N, R, LAYOUT, MODE, true>(
+        g, L, id, parity, mu, hb_offset, inj, pdl,
+        [&](uint32_t i, int e) { return ld_elem<R, LD_CG>(base + i + e * stride); },
+        [&](uint32_t i, int e, cx<R> v) { st_elem<R>(base + i + e * stride, v); });
 }
 
 template <class R> SUN_DEV cx<R> shfl_cx(cx<R> v, int src)
@@ -245,7 +262,7 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
     const LatDev& L = bv.lats[l];
     const Geom g = geom_of(L);
     const int first = (b - __ldg(bv.begin + l)) * ((int)(blockDim.x >> 5) * SPW) + (int)(threadIdx.x >> 5) * SPW;
-    if (first >= g.halfV) return;  // the whole warp is past the end
+    if (first >= g.halfV || lat_frozen(L)) return;  // the whole warp is past the end, or the lattice done
     const int id0 = first + slot;
     const bool valid = used && id0 < g.halfV;
     const int id = id0 < g.halfV ? id0 : g.halfV - 1;  // past the end: compute a copy, store nothing
@@ -378,6 +395,179 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
 }
 
 // ---------------------------------------------------------------------------
+// Tiled update for N >= 4 (full links): a CTA of N warps advances 32
+// half-sites, one per lane.  Warp w owns row w: it loads row w (up staple) or
+// column w (down staple) of the first factor of each staple straight into
+// registers, and the CTA stages the other two factors once in shared memory
+// (warp w loads their row w), so every link element is read from L2 exactly
+// once and every load is a 32-lane coalesced one.  Each warp then forms row w
+// of the six staple products with the row routines of k_update_rows (same
+// operations, same order: the same bits as k_update) and keeps row w of the
+// staple sum in registers.  The SU(2) subgroup updates run in warp 0, one
+// lane per site, streaming rows p and q of U and S from shared memory, so no
+// thread ever holds an N x N matrix: SU(6) needs no spills at a modest
+// register count, where one thread per site spills kilobytes.
+//
+// Shared memory (dynamic, tile_smem_bytes): B and D staging, N*N complex x
+// 32 sites each, then the staple sum S; U aliases the B/D staging once the
+// staples are summed.  Element e of a matrix sits at [e][lane]: a warp's
+// access to one element is 32 consecutive complex numbers (no bank
+// conflicts).
+constexpr int kTileSites = 32;
+template <int N, class R> constexpr int tile_smem_bytes() { return 3 * N * N * kTileSites * (int)sizeof(cx<R>); }
+
+template <int N, class R, int MODE>
+__global__ void __launch_bounds__(32 * N) k_update_tile(BatchView bv, int parity, int mu, unsigned hb_offset,
+                                                        InjView inj, int pdl)
+{
+    static_assert(N >= 4, "the tiled update serves N >= 4");
+    typedef cx<R> C;
+    extern __shared__ __align__(16) unsigned char tile_raw[];
+    C(*const Bs)[kTileSites] = reinterpret_cast<C(*)[kTileSites]>(tile_raw);
+    C(*const Ds)[kTileSites] = Bs + N * N;
+    C(*const Ss)[kTileSites] = Ds + N * N;
+    C(*const Us)[kTileSites] = Bs;  // after the staple sum
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;  // the row this warp owns
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    if (lat_frozen(L)) return;  // the whole CTA: no barrier reached yet
+    const int id0 = (b - __ldg(bv.begin + l)) * kTileSites + lane;
+    const bool valid = id0 < g.halfV;
+    const int id = valid ? id0 : g.halfV - 1;  // past the end: compute a copy, store nothing
+    const cx<R>* base = reinterpret_cast<const cx<R>*>(L.links);
+    const uint32_t V = (uint32_t)g.V, stride = 4u * V;
+
+    int x[4];
+    eo_coords(g, id, parity, x);
+    const int H = g.halfV;
+    const int sx = id + parity * H;
+    const int st[4] = {1, g.X[0], g.X[0] * g.X[1], g.X[0] * g.X[1] * g.X[2]};
+    const int lex = x[0] + st[1] * x[1] + st[2] * x[2] + st[3] * x[3];
+    const int xm = sel4(x, mu), Xm = sel4(g.X, mu), Sm = sel4(st, mu);
+    const int other = (1 - parity) * H;
+    const int sxpmu = (lex_step(lex, xm, Xm, Sm, 1) >> 1) + other;
+
+    const int dep = pdl ? ((mu + 3) & 3) : -1;  // as in k_update
+    if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    auto Bget = [&](int k, int j) { return Bs[k * N + j][lane]; };
+    auto Dget = [&](int k, int j) { return Ds[k * N + j][lane]; };
+    C Sr[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) Sr[j] = mkc<R>(0, 0);
+    // the order over nu of k_update: rotated for N = 4, ascending for N = 6
+    constexpr bool kRot = N <= 4;
+#pragma unroll 1
+    for (int kk = kRot ? 1 : 0; kk < 4; ++kk) {
+        const int nu = kRot ? ((mu + kk) & 3) : kk;
+        if (nu == mu) continue;
+        if (nu == dep) {
+            asm volatile("griddepcontrol.wait;" ::: "memory");
+            asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+        }
+        const int xn_ = sel4(x, nu), Xn_ = sel4(g.X, nu), Sn_ = sel4(st, nu);
+        const int lup = lex_step(lex, xn_, Xn_, Sn_, 1);
+        const int ldn = lex_step(lex, xn_, Xn_, Sn_, -1);
+        const int syp = (lup >> 1) + other;                               // x + nu
+        const int sy = (ldn >> 1) + other;                                // x - nu
+        const int sz = (lex_step(ldn, xm, Xm, Sm, 1) >> 1) + parity * H;  // x - nu + mu
+        C a[N], c[N];
+        // up: row w of U_nu(x) U_mu(x+nu) U_nu(x+mu)^dagger
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const uint32_t e = (uint32_t)(w * N + k) * stride;
+            a[k] = ld_elem<R, LD_CG>(base + (uint32_t)sx + nu * V + e);
+            Bs[w * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)syp + mu * V + e);
+            Ds[w * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sxpmu + nu * V + e);
+        }
+        __syncthreads();
+        rmul_g<N, R>(a, Bget, c);
+        racc_nd_g<N, R>(c, Dget, Sr);
+        __syncthreads();
+        // down: row w of U_nu(x-nu)^dagger U_mu(x-nu) U_nu(x-nu+mu)
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const uint32_t e = (uint32_t)(w * N + k) * stride;
+            a[k] = ld_elem<R, LD_CG>(base + (uint32_t)sy + nu * V + (uint32_t)(k * N + w) * stride);
+            Bs[w * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sy + mu * V + e);
+            Ds[w * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sz + nu * V + e);
+        }
+        __syncthreads();
+        rmul_dn_g<N, R>(a, Bget, c);
+        racc_g<N, R>(c, Dget, Sr);
+        __syncthreads();
+    }
+
+    cx<R>* wbase = reinterpret_cast<cx<R>*>(L.links);
+    const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        Ss[w * N + j][lane] = Sr[j];
+        Us[w * N + j][lane] = ld_elem<R, LD_CG>(wbase + own + (uint32_t)(w * N + j) * stride);
+    }
+    __syncthreads();
+    if (w == 0) {
+        // the subgroup sequence of overrelax_update / heatbath_update (N >= 4:
+        // blocks of U S^dagger recomputed from U and S), rows from shared memory
+        PhiloxStream<R> ph;
+        InjectedStream<R> is;
+        if constexpr (MODE == MODE_HB) ph.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
+        if constexpr (MODE == MODE_HB_INJECTED) {
+            is.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
+            is.left = inj.stride;
+            is.err = inj.err;
+        }
+        const R bon = (R)L.beta_over_n;
+#pragma unroll 1
+        for (int del = 1; del < N; ++del)
+#pragma unroll 1
+            for (int p = 0; p < N - del; ++p) {
+                const int q = p + del;
+                C a0 = mkc<R>(0, 0), a1 = a0, a2 = a0, a3 = a0;
+#pragma unroll
+                for (int j = 0; j < N; ++j) {
+                    const C up = Us[p * N + j][lane], uq = Us[q * N + j][lane];
+                    const C sp = Ss[p * N + j][lane], sq = Ss[q * N + j][lane];
+                    a0 = cfma_nc(up, sp, a0);
+                    a1 = cfma_nc(up, sq, a1);
+                    a2 = cfma_nc(uq, sp, a2);
+                    a3 = cfma_nc(uq, sq, a3);
+                }
+                R r[4] = {a0.re + a3.re, a1.im + a2.im, a1.re - a2.re, a0.im - a3.im};
+                R cq[4];
+                if constexpr (MODE == MODE_OR) {
+                    su2_overrelax_element(r, cq);
+                } else {
+                    R k = sqrt(qnorm2(r));
+                    R ap = bon * k;
+                    k = R(1) / k;
+                    r[0] *= k; r[1] *= k; r[2] *= k; r[3] *= k;
+                    R ad[4];
+                    if constexpr (MODE == MODE_HB) su2_draw<R>(ap, ph, ad);
+                    else su2_draw<R>(ap, is, ad);
+                    su2_mul_udag(ad, r, cq);
+                }
+                // su2_apply on rows p, q
+                const C m00 = mkc(cq[0], cq[3]), m01 = mkc(cq[2], cq[1]);
+                const C m10 = mkc(-cq[2], cq[1]), m11 = mkc(cq[0], -cq[3]);
+#pragma unroll
+                for (int j = 0; j < N; ++j) {
+                    const C up = Us[p * N + j][lane], uq = Us[q * N + j][lane];
+                    Us[p * N + j][lane] = cfma(m01, uq, m00 * up);
+                    Us[q * N + j][lane] = cfma(m11, uq, m10 * up);
+                }
+            }
+    }
+    __syncthreads();
+    if (valid) {
+#pragma unroll
+        for (int j = 0; j < N; ++j) st_elem<R>(wbase + own + (uint32_t)(w * N + j) * stride, Us[w * N + j][lane]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Link-wise kernels: work index w over 4V links, w = site * 4 + mu with
 // `site` in the lattice's storage order.
 template <int N, class R, int LAYOUT>
@@ -476,7 +666,9 @@ __global__ void __launch_bounds__(256) k_reunit(BatchView bv, int only_due)
     const int l = find_lat(bv, b);
     const LatDev& L = bv.lats[l];
     if (only_due) {
-        if (L.reunit_every <= 0) return;
+        // due after a sweep that advanced the lattice (not after the sweeps
+        // a lattice at its sweep limit sits out)
+        if (L.reunit_every <= 0 || L.state[2] == 0u) return;
         const unsigned sw = L.state[1];
         if (sw == 0u || (sw % (unsigned)L.reunit_every) != 0u) return;
     }
@@ -538,9 +730,11 @@ SUN_DEV void block_sum(double v, double* out, DD* sh)
 // finish (each CTA fences its partials, then counts itself in): the same
 // lane-strided compensated sums and shuffle tree as k_finalize_sum, so the
 // result is the same whichever CTA runs it.  The result goes straight to
-// out (host-mapped memory allowed); the counter is left at zero.
+// out (host-mapped memory allowed); the counter is left at zero.  slot (may
+// be null): a device counter; the results go to row *slot of out (nlat *
+// nvals doubles per row), so a replayed graph fills one row per replay.
 SUN_DEV void finalize_if_last(const BatchView& bv, int l, const double* partials, int nvals, double* out,
-                              unsigned* counters)
+                              unsigned* counters, const unsigned* slot)
 {
     __shared__ int last;
     __threadfence();
@@ -564,7 +758,8 @@ SUN_DEV void finalize_if_last(const BatchView& bv, int l, const double* partials
             d = dd_add(d, t);
         }
         d = dd_warp(d);
-        if (lane == 0) out[(size_t)l * nvals + v] = d.s + d.c;
+        const size_t row = slot ? (size_t)__ldcg(slot) * (size_t)bv.nlat * nvals : 0;
+        if (lane == 0) out[row + (size_t)l * nvals + v] = d.s + d.c;
     }
     if (lane == 0) counters[l] = 0u;
 }
@@ -638,7 +833,8 @@ SUN_DEV double plaquette_plane(const LatDev& L, const Geom& g, const int x[4], i
 }
 
 template <int N, class R, int LAYOUT>
-__global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partials, double* out, unsigned* counters)
+__global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partials, double* out, unsigned* counters,
+                                                    const unsigned* slot)
 {
     __shared__ DD sh[32];
     const int b = blockIdx.x;
@@ -671,7 +867,7 @@ __global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partial
     }
     block_sum(sp, partials + (size_t)b * 4, sh);
     block_sum(tp, partials + (size_t)b * 4 + 2, sh);
-    if (out) finalize_if_last(bv, l, partials, 2, out, counters);
+    if (out) finalize_if_last(bv, l, partials, 2, out, counters, slot);
 }
 
 template <int N> SUN_DEV void shfl_mat(Mat<N, double>& D, const Mat<N, double>& S, int src)
@@ -691,7 +887,8 @@ template <int N> SUN_DEV void shfl_mat(Mat<N, double>& D, const Mat<N, double>& 
 // in order by a shuffle tree, (P0 P1)(P2 P3)..., so the time chain is T / 8
 // products plus three joins instead of T products.
 template <int N, class R, int LAYOUT>
-__global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials, double* out, unsigned* counters)
+__global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials, double* out, unsigned* counters,
+                                                   const unsigned* slot)
 {
     __shared__ DD sh[32];
     const int b = blockIdx.x;
@@ -737,7 +934,7 @@ __global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials
     }
     block_sum(re, partials + (size_t)b * 4, sh);
     block_sum(im, partials + (size_t)b * 4 + 2, sh);
-    if (out) finalize_if_last(bv, l, partials, 2, out, counters);
+    if (out) finalize_if_last(bv, l, partials, 2, out, counters, slot);
 }
 
 // Planar Wilson loops W(r,t), r <= R, t <= T, averaged over the 3 spatial
@@ -947,12 +1144,12 @@ __global__ void __launch_bounds__(256) k_unpack(BatchView bv, double2* canon)
 // it on the stream (which must be the previous update phase).
 template <class K>
 cudaError_t launch_phase(K kernel, const BatchView& bv, int block, int parity, int mu, unsigned hb_offset,
-                         const InjView& inj, int pdl, cudaStream_t s)
+                         const InjView& inj, int pdl, cudaStream_t s, int smem = 0)
 {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)bv.nblocks);
     cfg.blockDim = dim3((unsigned)block);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = (size_t)smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -990,6 +1187,42 @@ cudaError_t Ops<N>::update_rows(int fp64, int layout, int mode, const BatchView&
     return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+// the tiled update's instance for (R, MODE), its shared memory opted in once
+template <int N, class R, int MODE> cudaError_t launch_tile(const BatchView& bv, int parity, int mu,
+                                                            unsigned hb_offset, const InjView& inj, int pdl,
+                                                            cudaStream_t s)
+{
+    constexpr int smem = tile_smem_bytes<N, R>();
+    static const cudaError_t attr =
+        smem > 48 * 1024
+            ? cudaFuncSetAttribute(k_update_tile<N, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+            : cudaSuccess;
+    if (attr != cudaSuccess) return attr;
+    return launch_phase(k_update_tile<N, R, MODE>, bv, 32 * N, parity, mu, hb_offset, inj, pdl, s, smem);
+}
+
+template <int N>
+cudaError_t Ops<N>::update_tile(int fp64, int layout, int mode, const BatchView& bv, int parity, int mu,
+                                unsigned hb_offset, const InjView& inj, int pdl, cudaStream_t s)
+{
+    if constexpr (N < 4) {
+        return cudaErrorInvalidValue;
+    } else {
+        if (layout != L_SOA) return cudaErrorInvalidValue;
+        cudaError_t e;
+        if (fp64) {
+            if (mode == MODE_OR) e = launch_tile<N, double, MODE_OR>(bv, parity, mu, hb_offset, inj, pdl, s);
+            else if (mode == MODE_HB) e = launch_tile<N, double, MODE_HB>(bv, parity, mu, hb_offset, inj, pdl, s);
+            else e = launch_tile<N, double, MODE_HB_INJECTED>(bv, parity, mu, hb_offset, inj, pdl, s);
+        } else {
+            if (mode == MODE_OR) e = launch_tile<N, float, MODE_OR>(bv, parity, mu, hb_offset, inj, pdl, s);
+            else if (mode == MODE_HB) e = launch_tile<N, float, MODE_HB>(bv, parity, mu, hb_offset, inj, pdl, s);
+            else e = launch_tile<N, float, MODE_HB_INJECTED>(bv, parity, mu, hb_offset, inj, pdl, s);
+        }
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
+}
+
 template <int N> cudaError_t Ops<N>::cold(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s)
 {
 #define CALL(R_, L_) k_cold<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv)
@@ -1017,9 +1250,9 @@ cudaError_t Ops<N>::reunit(int fp64, int layout, const BatchView& bv, int block,
 
 template <int N>
 cudaError_t Ops<N>::plaquette(int fp64, int layout, const BatchView& bv, int block, double* partials,
-                              double* out, unsigned* counters, cudaStream_t s)
+                              double* out, unsigned* counters, const unsigned* slot, cudaStream_t s)
 {
-#define CALL(R_, L_) k_plaquette<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials, out, counters)
+#define CALL(R_, L_) k_plaquette<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials, out, counters, slot)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
     return cudaGetLastError();
@@ -1027,9 +1260,9 @@ cudaError_t Ops<N>::plaquette(int fp64, int layout, const BatchView& bv, int blo
 
 template <int N>
 cudaError_t Ops<N>::polyakov(int fp64, int layout, const BatchView& bv, int block, double* partials,
-                             double* out, unsigned* counters, cudaStream_t s)
+                             double* out, unsigned* counters, const unsigned* slot, cudaStream_t s)
 {
-#define CALL(R_, L_) k_polyakov<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials, out, counters)
+#define CALL(R_, L_) k_polyakov<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials, out, counters, slot)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
     return cudaGetLastError();

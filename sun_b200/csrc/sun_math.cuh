@@ -21,13 +21,19 @@ template <class R> struct cx { R re, im; };
 template <class R> SUN_HD cx<R> mkc(R a, R b) { cx<R> c; c.re = a; c.im = b; return c; }
 template <class R> SUN_HD cx<R> operator+(cx<R> a, cx<R> b) { return mkc(a.re + b.re, a.im + b.im); }
 template <class R> SUN_HD cx<R> operator-(cx<R> a, cx<R> b) { return mkc(a.re - b.re, a.im - b.im); }
+// The library is compiled without implicit multiply-add contraction
+// (-fmad=false): every fused operation is written out as fma(), so each
+// kernel rounds exactly as its source says and kernels that perform the same
+// operations give the same bits, whatever the compiler does around them.
 template <class R> SUN_HD cx<R> operator*(cx<R> a, cx<R> b)
 {
-    return mkc(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+    return mkc(fma(a.re, b.re, -(a.im * b.im)), fma(a.re, b.im, a.im * b.re));
 }
 template <class R> SUN_HD cx<R> operator*(R s, cx<R> a) { return mkc(s * a.re, s * a.im); }
 template <class R> SUN_HD cx<R> cconj(cx<R> a) { return mkc(a.re, -a.im); }
-template <class R> SUN_HD R cnorm2(cx<R> a) { return a.re * a.re + a.im * a.im; }
+template <class R> SUN_HD R cnorm2(cx<R> a) { return fma(a.re, a.re, a.im * a.im); }
+// |r|^2 of a quaternion 4-vector
+template <class R> SUN_HD R qnorm2(const R r[4]) { return fma(r[3], r[3], fma(r[2], r[2], fma(r[1], r[1], r[0] * r[0]))); }
 // acc + a*b, acc + conj(a)*b, acc + a*conj(b) as FMA chains
 template <class R> SUN_HD cx<R> cfma(cx<R> a, cx<R> b, cx<R> acc)
 {
@@ -238,6 +244,50 @@ template <int N, class R> SUN_DEV void racc_dn(const cx<R> a[N], const Mat<N, R>
         s[j] = t;
     }
 }
+// The same four row routines with the right factor B read through an
+// accessor B(k, j) (e.g. a matrix staged in shared memory): the same
+// operations in the same order, so the same bits.
+template <int N, class R, class G> SUN_DEV void rmul_g(const cx<R> a[N], G&& B, cx<R> c[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> s = a[0] * B(0, j);
+#pragma unroll
+        for (int k = 1; k < N; ++k) s = cfma(a[k], B(k, j), s);
+        c[j] = s;
+    }
+}
+template <int N, class R, class G> SUN_DEV void rmul_dn_g(const cx<R> a[N], G&& B, cx<R> c[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> s = mkc<R>(0, 0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) s = cfma_cn(a[k], B(k, j), s);
+        c[j] = s;
+    }
+}
+template <int N, class R, class G> SUN_DEV void racc_nd_g(const cx<R> a[N], G&& B, cx<R> s[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> t = s[j];
+#pragma unroll
+        for (int k = 0; k < N; ++k) t = cfma_nc(a[k], B(j, k), t);
+        s[j] = t;
+    }
+}
+template <int N, class R, class G> SUN_DEV void racc_g(const cx<R> a[N], G&& B, cx<R> s[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> t = s[j];
+#pragma unroll
+        for (int k = 0; k < N; ++k) t = cfma(a[k], B(k, j), t);
+        s[j] = t;
+    }
+}
+
 // row 2 of an SU(3) matrix from rows 0, 1 -- rebuild12
 template <class R> SUN_DEV void rebuild12_row(const cx<R> a[3], const cx<R> b[3], cx<R> c[3])
 {
@@ -350,10 +400,10 @@ template <int N, class R> SUN_DEV void su2_apply(Mat<N, R>& L, int p, int q, con
 // a * r^dagger on quaternion 4-vectors -- mulsu2UVDagger (msu2.h:212-219)
 template <class R> SUN_DEV void su2_mul_udag(const R a[4], const R r[4], R b[4])
 {
-    b[0] = a[0] * r[0] + a[1] * r[1] + a[2] * r[2] + a[3] * r[3];
-    b[1] = a[1] * r[0] - a[0] * r[1] + a[2] * r[3] - a[3] * r[2];
-    b[2] = a[2] * r[0] - a[0] * r[2] + a[3] * r[1] - a[1] * r[3];
-    b[3] = a[3] * r[0] - a[0] * r[3] + a[1] * r[2] - a[2] * r[1];
+    b[0] = fma(a[3], r[3], fma(a[2], r[2], fma(a[1], r[1], a[0] * r[0])));
+    b[1] = fma(-a[3], r[2], fma(a[2], r[3], fma(-a[0], r[1], a[1] * r[0])));
+    b[2] = fma(-a[1], r[3], fma(a[3], r[1], fma(-a[0], r[2], a[2] * r[0])));
+    b[3] = fma(-a[2], r[1], fma(a[1], r[2], fma(-a[0], r[3], a[3] * r[0])));
 }
 
 // SU(3) third row from the first two: row2 = conj(row0 x row1) --

@@ -13,10 +13,24 @@ struct LatDev {
     int V, halfV;
     double beta_over_n;       // beta / N (constants.cu:443)
     unsigned long long seed;  // Philox key
-    unsigned int* state;      // device counters: [0] heatbath passes, [1] sweeps
+    unsigned int* state;      // device counters: [0] heatbath passes, [1] sweeps, [2] 1 if the
+                              // last counted sweep advanced the lattice (see sweep_limit)
     int reunit_every;         // reunitarize when sweeps % reunit_every == 0 (0: never)
     int evenodd;              // storage order: 1 even/odd, 0 lexicographic
+    unsigned sweep_limit;     // 0: none; else the lattice is left unchanged once its sweep
+                              // counter reaches the limit (the update kernels skip it, the
+                              // counters and the reunitarization schedule stop)
 };
+// A lattice whose sweep counter reached its limit: update launches skip it.
+__host__ __device__ inline bool lat_frozen(const LatDev& L)
+{
+#ifdef __CUDA_ARCH__
+    return L.sweep_limit != 0u && __ldcg(L.state + 1) >= L.sweep_limit;
+#else
+    (void)L;
+    return false;
+#endif
+}
 
 // A launch over several lattices of one class (same N, precision, layout):
 // CTA b works on lattice l with begin[l] <= b < begin[l+1].
@@ -36,6 +50,7 @@ struct InjView {
 };
 
 enum UpdateMode { MODE_HB = 0, MODE_HB_INJECTED = 1, MODE_OR = 2 };
+
 
 // Work per lattice a launch maps CTAs onto.
 // work items per lattice of a launch: half-sites, sites, spatial sites,
@@ -65,6 +80,11 @@ template <int N> struct Ops {
     static cudaError_t update_rows(int fp64, int layout, int mode, const BatchView& bv, int block,
                                    int parity, int mu, unsigned hb_offset, const InjView& inj, int pdl,
                                    cudaStream_t s);
+    // the same phase with a CTA of N warps per 32 half-sites and the staple
+    // factors staged in shared memory (k_update_tile; N >= 4, full links);
+    // the same bits as update()
+    static cudaError_t update_tile(int fp64, int layout, int mode, const BatchView& bv, int parity, int mu,
+                                   unsigned hb_offset, const InjView& inj, int pdl, cudaStream_t s);
     static cudaError_t cold(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
     static cudaError_t hot(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
     // FP64 reunitarization; only_due: skip lattices whose sweep counter is not
@@ -75,11 +95,12 @@ template <int N> struct Ops {
     // unitarity 1 (max); partial layout [block][value][sum, compensation]
     // plaquette and polyakov: with out non-null, the last CTA of each
     // lattice also finalizes its sums into out[2 l .. 2 l + 1] (counters: one
-    // zeroed unsigned per lattice, left at zero)
+    // zeroed unsigned per lattice, left at zero); with slot non-null, into
+    // row *slot of out (2 nlat doubles per row)
     static cudaError_t plaquette(int fp64, int layout, const BatchView& bv, int block, double* partials,
-                                 double* out, unsigned* counters, cudaStream_t s);
+                                 double* out, unsigned* counters, const unsigned* slot, cudaStream_t s);
     static cudaError_t polyakov(int fp64, int layout, const BatchView& bv, int block, double* partials,
-                                double* out, unsigned* counters, cudaStream_t s);
+                                double* out, unsigned* counters, const unsigned* slot, cudaStream_t s);
     static cudaError_t wilson(int fp64, int layout, const BatchView& bv, int block, int R, int T,
                               double* partials, cudaStream_t s);
     static cudaError_t unitarity(int fp64, int layout, const BatchView& bv, int block, double* partials,
@@ -119,6 +140,8 @@ cudaError_t launch_finalize_sum(const BatchView& bv, const double* partials, int
                                 cudaStream_t s);
 cudaError_t launch_finalize_max(const BatchView& bv, const double* partials, double* out, cudaStream_t s);
 cudaError_t launch_end_sweep(const LatDev* lats, int nlat, unsigned n_hb, unsigned inc, cudaStream_t s);
+// *slot += 1 (the row counter of replayed measurements)
+cudaError_t launch_bump(unsigned* slot, cudaStream_t s);
 // message returned by sun_last_error_string(NULL)
 void set_global_error(const char* msg);
 

@@ -184,6 +184,46 @@ def test_heatbath_philox_matches_oracle(ctx, case):
     assert g.rng_state()[1] == 1
 
 
+LARGE = [  # SU(3) lattices on the benchmark's code paths
+    ((16, 16, 16, 16), "f32", 1), ((16, 16, 16, 16), "f64", 0),
+    ((16, 16, 16, 32), "f32", 1), ((16, 16, 16, 32), "f64", 0),
+]
+
+
+@pytest.mark.parametrize("dims,prec,lay", LARGE,
+                         ids=[f"{'x'.join(map(str, d))}-{p}-{['SOA', 'SOA12'][l]}" for d, p, l in LARGE])
+def test_large_lattice_passes_and_measurements_match_oracle(ctx, dims, prec, lay):
+    """An overrelaxation pass, a heatbath pass and the measurements on 16^4
+    and 16^3 x 32 lattices: the update kernel with one thread per half-site
+    (32-bit element offsets over 4V links), the plaquette's per-site branch
+    (V = 2^17 sites, the branch of the 32^4 benchmark) and its (site, plane)
+    branch below that volume.  The start is thermalized (two oracle sweeps
+    from Haar): on a Haar-random configuration some staple sums nearly
+    vanish, and FP32 rounding of a nearly vanishing SU(2) block turns the
+    overrelaxation reflection by up to ~1e-3."""
+    from sun_b200 import HeatBath, OnePolyakovLoop, OverRelaxation, PlaquetteCUB
+    X = list(dims)
+    U = O.hot(3, X, 9)
+    O.sweeps(U, X, 6.0, 1, 1, 2, seed=9)
+    g = _make(ctx, 3, dims, prec, lay, beta=6.0, seed=31)
+    g.Set(U)
+    ref = g.Get()
+    OverRelaxation(g).Run(1)
+    O.sweeps(ref, X, 6.0, 0, 1, 1)
+    got = g.Get()
+    assert np.abs(got - ref).max() < _tol(prec, lay)
+    ref = got
+    HeatBath(g).Run(1)
+    O.sweeps(ref, X, 6.0, 1, 0, 1, mode=O.RNG_PHILOX64 if prec == "f64" else O.RNG_PHILOX32, seed=31)
+    got = g.Get()
+    frac, d = _mismatch(got, ref, _tol(prec, lay))
+    assert frac == 0.0 if prec == "f64" else frac < 0.01, (frac, d.max())
+    p, l = PlaquetteCUB(g).Run(), OnePolyakovLoop(g).Run()
+    po, lo = O.plaquette(got, X), O.polyakov(got, X)
+    assert abs(p.real - po[0]) < 1e-12 and abs(p.imag - po[1]) < 1e-12
+    assert abs(l.real - lo[0]) < 1e-12 and abs(l.imag - lo[1]) < 1e-12
+
+
 @pytest.mark.parametrize("case", [c for c in ALL if c[1] == (4, 4, 4, 4)], ids=_ids)
 def test_heatbath_injected_matches_oracle(ctx, case):
     import torch
@@ -408,12 +448,10 @@ def test_server_result_independent_of_mix(ctx):
         res1 += s1.step()
     s2 = Server(ctx, max_active=8)
     s2.submit(make_job(N=2, dims=(4, 4, 4, 4), beta=2.2, sweeps=3, seed=3))
-    s2.step()
-    s2.step()
+    res2 = s2.step() + s2.step()
     jid = s2.submit(job)
     s2.submit(make_job(N=4, dims=(4, 4, 4, 4), beta=10.5, sweeps=9, seed=4, observables=3))
     s2.submit(make_job(N=3, dims=(6, 6, 6, 6), beta=6.0, sweeps=2, seed=5))
-    res2 = []
     for _ in range(20):
         res2 += s2.step()
     r2 = [r for r in res2 if r["id"] == jid][0]
@@ -422,6 +460,70 @@ def test_server_result_independent_of_mix(ctx):
     assert r1["plaquette"] == r2["plaquette"] and r1["polyakov"] == r2["polyakov"]
     assert r1["wilson"] == r2["wilson"]
     assert len(res2) == 4
+
+
+def test_sweep_limit_stops_each_lattice_at_its_count(ctx):
+    """A batch swept more often than some of its lattices need: each lattice
+    with a sweep limit ends exactly as after its own count of sweeps alone --
+    links, RNG counters and the reunitarization schedule (every 2 sweeps)."""
+    from sun_b200 import Batch, Sweep
+    batch, alone, mixed = Batch(ctx), [], []
+    for i, (d, limit, N, prec, lay) in enumerate([((4, 4, 4, 8), 3, 3, "f32", 1), ((6, 6, 6, 6), 5, 3, "f64", 0),
+                                                   ((4, 4, 4, 4), 1, 4, "f32", 0), ((8, 8, 8, 8), 0, 3, "f32", 1),
+                                                   ((4, 4, 4, 4), 4, 2, "f32", 0)]):
+        beta = {2: 2.2, 3: 5.9, 4: 10.5}[N]
+        a = _make(ctx, N, d, prec, lay, seed=60 + i, beta=beta, reunit_every=2)
+        b = _make(ctx, N, d, prec, lay, seed=60 + i, beta=beta, reunit_every=2)
+        a.Init(hot=True)
+        b.Init(hot=True)
+        b.set_sweep_limit(limit)
+        Sweep(a, 1, 4, limit or 7)
+        alone.append(a)
+        mixed.append(b)
+        batch.add(b)
+    batch.sweep(1, 4, 2)
+    batch.sweep(1, 4, 5, graph=True)
+    for a, b in zip(alone, mixed):
+        assert np.array_equal(a.get_image(), b.get_image())
+        assert a.rng_state() == b.rng_state()
+    batch.close()
+
+
+def test_batch_wilson_loops_match_each_lattice(ctx):
+    from sun_b200 import Batch, WilsonLoop
+    batch, lats = Batch(ctx), []
+    for i, (N, d, prec, lay) in enumerate([(3, (6, 6, 6, 10), "f32", 1), (4, (6, 6, 6, 6), "f32", 0),
+                                            (3, (8, 8, 8, 8), "f64", 0), (2, (6, 6, 6, 8), "f64", 0)]):
+        g = _make(ctx, N, d, prec, lay, seed=80 + i)
+        g.Init(hot=True)
+        batch.add(g)
+        lats.append(g)
+    w = batch.wilson_loops(4, 4)
+    for i, g in enumerate(lats):
+        assert np.array_equal(w[i], WilsonLoop(g, 4, 4))
+    batch.close()
+
+
+def test_server_budget_defaults_to_the_context_budget():
+    """sun_config.hbm_budget_bytes is the server's admission budget: a job
+    whose footprint exceeds it is refused with SUN_ERR_CAPACITY."""
+    from sun_b200 import Context, Server, job_footprint, make_job
+    job = make_job(N=3, dims=(8, 8, 8, 8), beta=5.8, sweeps=1, seed=1)
+    small = job_footprint(job) - 1
+    with Context(0, hbm_budget_bytes=small) as c:
+        s = Server(c, max_active=4)
+        s.submit(job)
+        res = s.step()
+        assert len(res) == 1 and res[0]["status"] == 7
+        s.close()
+    with Context(0, hbm_budget_bytes=job_footprint(job)) as c:
+        s = Server(c, max_active=4)
+        s.submit(job)
+        res = []
+        for _ in range(5):
+            res += s.step()
+        assert len(res) == 1 and res[0]["status"] == 0
+        s.close()
 
 
 def test_batch_of_uneven_shapes_with_graph(ctx):

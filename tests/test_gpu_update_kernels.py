@@ -1,11 +1,13 @@
-"""The two update kernels give the same bits.
+"""The three update kernels give the same bits.
 
 k_update runs one thread per half-site; k_update_rows, which the engine takes
 for small lattices of N >= 4 and of SU(3) with FP64 full links, spreads each
-half-site over N lanes.  Every element of the staple sum and the update goes
-through the same operations in both, so sweeps and heatbath passes with
-injected uniforms must agree bit for bit on every class, shape and mode,
-whichever kernel the size rule picks.
+half-site over N lanes; k_update_tile, which it takes for larger lattices of
+N >= 4, runs N warps per 32 half-sites with the staple factors staged in
+shared memory and the SU(2) updates streamed from it.  Every element of the
+staple sum and the update goes through the same operations in all three, so
+sweeps and heatbath passes with injected uniforms must agree bit for bit on
+every class, shape and mode, whichever kernel the size rule picks.
 The oracle parity tests therefore hold for both kernels; the overrelaxation
 and injected-heatbath parity of each is also checked here directly.
 """
@@ -53,10 +55,12 @@ def _context(kind):
 
 @pytest.fixture(scope="module")
 def ctxs():
-    sites, rows = _context("sites"), _context("rows")
-    yield sites, rows
-    sites.close()
-    rows.close()
+    # "tile" runs k_update_tile where it applies (N >= 4) and the size rule
+    # elsewhere
+    out = (_context("sites"), _context("rows"), _context("tile"))
+    yield out
+    for c in out:
+        c.close()
 
 
 BETA = {2: 2.3, 3: 5.8, 4: 10.5, 6: 25.0}
@@ -84,11 +88,12 @@ def _uniforms(N, dims, seed):
 def test_sweeps_identical(ctxs, case):
     from sun_b200 import Sweep
     N, prec, lay, dims = case
-    a, b = _pair(ctxs, N, prec, lay, dims, seed=31, reunit_every=2)
-    Sweep(a, 1, 4, 3)
-    Sweep(b, 1, 4, 3)
-    assert np.array_equal(a.get_image(), b.get_image())
-    assert a.rng_state() == b.rng_state()
+    gs = _pair(ctxs, N, prec, lay, dims, seed=31, reunit_every=2)
+    for g in gs:
+        Sweep(g, 1, 4, 3)
+    for g in gs[1:]:
+        assert np.array_equal(gs[0].get_image(), g.get_image())
+        assert gs[0].rng_state() == g.rng_state()
 
 
 @pytest.mark.parametrize("case", [c for c in CASES if c[3] == (4, 6, 8, 4)], ids=_ids)
@@ -96,16 +101,23 @@ def test_injected_heatbath_identical(ctxs, case):
     import torch
     from sun_b200 import HeatBath
     N, prec, lay, dims = case
-    a, b = _pair(ctxs, N, prec, lay, dims, seed=8)
+    gs = _pair(ctxs, N, prec, lay, dims, seed=8)
     u, stride = _uniforms(N, dims, 4)
     du = torch.tensor(u, dtype=torch.float64, device="cuda")
-    HeatBath(a).RunInjected(du.data_ptr(), stride)
-    HeatBath(b).RunInjected(du.data_ptr(), stride)
-    assert np.array_equal(a.get_image(), b.get_image())
+    for g in gs:
+        HeatBath(g).RunInjected(du.data_ptr(), stride)
+    for g in gs[1:]:
+        assert np.array_equal(gs[0].get_image(), g.get_image())
 
 
-@pytest.mark.parametrize("kernel", [0, 1], ids=["sites", "rows"])
-@pytest.mark.parametrize("N,prec,lay", [(3, "f64", 0), (3, "f32", 1), (4, "f64", 0), (6, "f32", 0)])
+EACH = [(k, N, prec, lay) for k in (0, 1, 2)
+        for N, prec, lay in [(3, "f64", 0), (3, "f32", 1), (4, "f64", 0), (4, "f32", 0), (6, "f32", 0),
+                             (6, "f64", 0)]
+        if k < 2 or N >= 4]
+
+
+@pytest.mark.parametrize("kernel,N,prec,lay", EACH,
+                         ids=[f"{['sites', 'rows', 'tile'][k]}-N{N}-{p}-{['SOA', 'SOA12'][l]}" for k, N, p, l in EACH])
 def test_each_kernel_matches_oracle(ctxs, kernel, N, prec, lay):
     """One overrelaxation pass, then one heatbath pass with injected
     uniforms, against the oracle per link."""
@@ -153,16 +165,18 @@ def test_batch_graph_with_one_mode(ctxs):
         batch.close()
 
 
-@pytest.mark.parametrize("dims,prec,lay", [((4, 4, 4, 8), "f32", 1), ((8, 8, 8, 8), "f64", 0),
-                                           ((16, 16, 16, 16), "f32", 1), ((8, 8, 8, 8), "f32", 0)])
-def test_overlapped_phases_are_deterministic(ctx, dims, prec, lay):
+@pytest.mark.parametrize("N,dims,prec,lay", [(3, (4, 4, 4, 8), "f32", 1), (3, (8, 8, 8, 8), "f64", 0),
+                                             (3, (16, 16, 16, 16), "f32", 1), (3, (8, 8, 8, 8), "f32", 0),
+                                             (4, (16, 16, 16, 16), "f32", 0), (6, (12, 12, 12, 12), "f64", 0)])
+def test_overlapped_phases_are_deterministic(ctx, N, dims, prec, lay):
     """Consecutive phases overlap (programmatic dependent launch); the same
     passes on the same links must still give the same bits on every run --
-    a read served from a stale cache line would not."""
+    a read served from a stale cache line would not.  The SU(4) and SU(6)
+    cases run the tiled kernel (by size)."""
     from sun_b200 import HeatBath, OverRelaxation, Sweep, gauge
     imgs = []
     for _ in range(3):
-        g = gauge(ctx, N=3, dims=dims, beta=6.0, atype=lay, evenodd=True, prec=prec, seed=1234)
+        g = gauge(ctx, N=N, dims=dims, beta=BETA[N], atype=lay, evenodd=True, prec=prec, seed=1234)
         g.Init(hot=True)
         for _ in range(2):
             HeatBath(g).Run(1)
