@@ -242,7 +242,13 @@ sun_status sun_batch_destroy(sun_batch *b);
 sun_status sun_batch_add(sun_batch *b, sun_lattice *lat);
 sun_status sun_batch_remove(sun_batch *b, sun_lattice *lat);
 sun_status sun_batch_size(const sun_batch *b, int *n);
-/* use_graph: capture one sweep into a CUDA graph and replay it */
+/* use_graph: SUN_BATCH_GRAPH captures one sweep into a CUDA graph and replays
+ * it (the classes as parallel branches; direct launches fork them onto
+ * parallel streams the same way); | SUN_BATCH_NO_WAIT returns once the
+ * sweeps are queued on `stream` -- the caller synchronizes it before reading
+ * or changing the batch's lattices */
+#define SUN_BATCH_GRAPH 1
+#define SUN_BATCH_NO_WAIT 2
 sun_status sun_batch_sweep(sun_batch *b, int n_hb, int n_or, int n_sweeps, int use_graph, void *stream);
 /* out[2*i], out[2*i+1] for the i-th lattice in insertion order */
 sun_status sun_batch_plaquette(sun_batch *b, double *out, void *stream);

@@ -1605,9 +1605,18 @@ sun_status sun_batch_sweep(sun_batch* b, int n_hb, int n_or, int n_sweeps, int u
         b->regroup();
         cudaStream_t s = S(b->ctx, stream);
         if (b->order.empty() || n_sweeps == 0) return;
-        if (!use_graph) {
-            for (int i = 0; i < n_sweeps; ++i) batch_one_sweep(b, n_hb, n_or, s);
-            ck(cudaStreamSynchronize(s), "batch sweep");
+        const bool wait = !(use_graph & SUN_BATCH_NO_WAIT);
+        if (!(use_graph & SUN_BATCH_GRAPH)) {
+            // tables first: their uploads synchronise, which a branch stream
+            // must not do in the middle of a sweep
+            for (auto& g : b->groups) {
+                if (g->lats.empty()) continue;
+                if (n_hb > 0) upd_view(*g, update_block(b->ctx, *g, MODE_HB, s), s);
+                if (n_or > 0) upd_view(*g, update_block(b->ctx, *g, MODE_OR, s), s);
+                g->view(WORK_LINKS, b->ctx->blk_links, s);
+            }
+            for (int i = 0; i < n_sweeps; ++i) batch_one_sweep(b, n_hb, n_or, s, true);
+            if (wait) ck(cudaStreamSynchronize(s), "batch sweep");
             return;
         }
         if (!b->graph || b->graph_hb != n_hb || b->graph_or != n_or) {
@@ -1641,7 +1650,7 @@ sun_status sun_batch_sweep(sun_batch* b, int n_hb, int n_or, int n_sweeps, int u
             b->graph_or = n_or;
         }
         for (int i = 0; i < n_sweeps; ++i) ck(cudaGraphLaunch(b->graph, s), "graph launch");
-        ck(cudaStreamSynchronize(s), "batch sweep");
+        if (wait) ck(cudaStreamSynchronize(s), "batch sweep");
     });
 }
 

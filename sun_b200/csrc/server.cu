@@ -103,12 +103,22 @@ struct sun_server {
     // sweeps per step: about step_target_s of GPU work, at most k_max
     double step_target_s = 0.05, sweep_s = 0.0;
     int k_max = 16;
+    // the step's sweeps and measurements run on `work` while new jobs'
+    // lattices are set up on `side`; t_sweep brackets the sweeps
+    cudaStream_t work = nullptr, side = nullptr;
+    cudaEvent_t t_sweep[2] = {nullptr, nullptr};
+    std::vector<Active> admitted;  // set up during the last step, not yet in a batch
 
     ~sun_server()
     {
         for (auto& a : active) sun_lattice_destroy(a.lat);
+        for (auto& a : admitted) sun_lattice_destroy(a.lat);
         for (auto& kv : batches) sun_batch_destroy(kv.second);
         if (retiring) sun_batch_destroy(retiring);
+        if (side) cudaStreamDestroy(side);
+        if (work) cudaStreamDestroy(work);
+        for (auto e : t_sweep)
+            if (e) cudaEventDestroy(e);
     }
     double now() const { return clock_s() - t0; }
     sun_batch* batch_for(const sun_job& j)
@@ -160,6 +170,12 @@ sun_status sun_server_create(sun_ctx* ctx, int max_active, sun_server** out)
         delete s;
         return SUN_ERR_INVALID_ARG;
     }
+    if (cudaStreamCreateWithFlags(&s->work, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&s->t_sweep[0]) != cudaSuccess || cudaEventCreate(&s->t_sweep[1]) != cudaSuccess) {
+        delete s;
+        return SUN_ERR_CUDA;
+    }
     s->t0 = clock_s();
     *out = s;
     return SUN_OK;
@@ -202,7 +218,7 @@ sun_status sun_server_pending(const sun_server* s, int* queued, int* active)
 {
     if (!s) return SUN_ERR_INVALID_ARG;
     if (queued) *queued = (int)s->queue.size();
-    if (active) *active = (int)s->active.size();
+    if (active) *active = (int)(s->active.size() + s->admitted.size());
     return SUN_OK;
 }
 
@@ -210,7 +226,27 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
 {
     if (!s || !n_done || (cap > 0 && !out)) return SUN_ERR_INVALID_ARG;
     auto emit = [&](const sun_result& r) { s->outbox.push_back(r); };
-    // 1. admission
+    // 1. queue up to K sweeps of every active job, batched per (n_hb, n_or),
+    // on the work stream without waiting; a job with fewer sweeps left
+    // stops at its own count (device-side limit)
+    int left_max = 0;
+    for (auto& a : s->active) left_max = std::max(left_max, a.remaining);
+    int k = 0;
+    if (left_max > 0) {
+        k = s->sweep_s > 0 ? (int)(s->step_target_s / s->sweep_s + 0.5) : 1;
+        k = std::max(1, std::min(std::min(k, s->k_max), left_max));
+        cudaEventRecord(s->t_sweep[0], s->work);
+        for (auto& kv : s->batches) {
+            int n = 0;
+            sun_batch_size(kv.second, &n);
+            if (n == 0) continue;
+            sun_status st = sun_batch_sweep(kv.second, kv.first.first, kv.first.second, k, SUN_BATCH_NO_WAIT, s->work);
+            if (st != SUN_OK) return st;
+        }
+    }
+    // 2. meanwhile admit queued jobs: their lattices are allocated and
+    // initialized on the side stream while the GPU sweeps, and join their
+    // batches after this step's sweeps
     {
         std::vector<size_t> fp;
         for (auto& p : s->queue) {
@@ -219,15 +255,15 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
             fp.push_back(f);
         }
         int n_admit = 0;
-        sun_admit_count(fp.data(), (int)fp.size(), s->budget, s->used, s->max_active - (int)s->active.size(),
-                        &n_admit);
+        const int slots = s->max_active - (int)(s->active.size() + s->admitted.size());
+        sun_admit_count(fp.data(), (int)fp.size(), s->budget, s->used, slots, &n_admit);
         for (int i = 0; i < n_admit; ++i) {
             sun_server::Pending p = s->queue.front();
             const sun_job& j = p.job;
             sun_lattice_params lp;
             memset(&lp, 0, sizeof lp);
             lp.ncolors = j.ncolors;
-            for (int k = 0; k < 4; ++k) lp.dims[k] = j.dims[k];
+            for (int d = 0; d < 4; ++d) lp.dims[d] = j.dims[d];
             lp.beta = j.beta;
             lp.layout = j.layout;
             lp.order = SUN_EVEN_ODD;
@@ -238,11 +274,9 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
             sun_status st = sun_lattice_create(s->ctx, &lp, &lat);
             if (st == SUN_ERR_OUT_OF_MEMORY) break;  // retry at the next step
             s->queue.pop_front();
-            if (st == SUN_OK) st = j.hot_start ? sun_lattice_init_hot(lat, nullptr) : sun_lattice_init_cold(lat, nullptr);
+            if (st == SUN_OK) st = j.hot_start ? sun_lattice_init_hot(lat, s->side) : sun_lattice_init_cold(lat, s->side);
             if (st == SUN_OK) st = sun_lattice_set_sweep_limit(lat, (uint32_t)j.sweeps);
-            sun_batch* b = (st == SUN_OK && j.sweeps > 0) ? s->batch_for(j) : nullptr;
-            if (st == SUN_OK && j.sweeps > 0 && !b) st = SUN_ERR_CUDA;
-            if (st == SUN_OK && b) st = sun_batch_add(b, lat);
+            if (st == SUN_OK && j.sweeps > 0 && !s->batch_for(j)) st = SUN_ERR_CUDA;
             if (st != SUN_OK) {
                 if (lat) sun_lattice_destroy(lat);
                 emit(blank_result(p.id, st, p.submit_s));
@@ -257,29 +291,20 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
             a.start_s = s->now();
             a.bytes = fp[i];
             s->used += a.bytes;
-            s->active.push_back(a);
+            s->admitted.push_back(a);
         }
     }
-    // 2. up to K sweeps of every active job, batched per (n_hb, n_or); a job
-    // with fewer sweeps left stops at its own count (device-side limit)
-    int left_max = 0;
-    for (auto& a : s->active) left_max = std::max(left_max, a.remaining);
-    if (left_max > 0) {
-        int k = s->sweep_s > 0 ? (int)(s->step_target_s / s->sweep_s + 0.5) : 1;
-        k = std::max(1, std::min(std::min(k, s->k_max), left_max));
-        const double ts = clock_s();
-        for (auto& kv : s->batches) {
-            int n = 0;
-            sun_batch_size(kv.second, &n);
-            if (n == 0) continue;
-            sun_status st = sun_batch_sweep(kv.second, kv.first.first, kv.first.second, k, 1, nullptr);
-            if (st != SUN_OK) return st;
-        }
-        const double per = (clock_s() - ts) / k;
+    // 3. the sweeps done: seconds per sweep (CUDA events) for the next K
+    if (k > 0) {
+        cudaEventRecord(s->t_sweep[1], s->work);
+        if (cudaEventSynchronize(s->t_sweep[1]) != cudaSuccess) return SUN_ERR_CUDA;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, s->t_sweep[0], s->t_sweep[1]);
+        const double per = 1e-3 * ms / k;
         s->sweep_s = s->sweep_s > 0 ? 0.5 * (s->sweep_s + per) : per;
         for (auto& a : s->active) a.remaining = std::max(0, a.remaining - k);
     }
-    // 3. measure the finished jobs together (one launch per class and
+    // 4. measure the finished jobs together (one launch per class and
     // observable), then retire them
     std::vector<sun_server::Active> keep, fin;
     for (auto& a : s->active) (a.remaining > 0 ? keep : fin).push_back(a);
@@ -300,9 +325,9 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
             for (size_t i : idx) sun_batch_add(s->retiring, fin[i].lat);
             const int nv = bit == 4 ? 2 * (R + 1) * (T + 1) : 2;
             std::vector<double> out(nv * idx.size());
-            sun_status st = bit == 1   ? sun_batch_plaquette(s->retiring, out.data(), nullptr)
-                            : bit == 2 ? sun_batch_polyakov(s->retiring, out.data(), nullptr)
-                                       : sun_batch_wilson_loops(s->retiring, R, T, out.data(), nullptr);
+            sun_status st = bit == 1   ? sun_batch_plaquette(s->retiring, out.data(), s->work)
+                            : bit == 2 ? sun_batch_polyakov(s->retiring, out.data(), s->work)
+                                       : sun_batch_wilson_loops(s->retiring, R, T, out.data(), s->work);
             for (size_t q = 0; q < idx.size(); ++q) {
                 const size_t i = idx[q];
                 if (st != SUN_OK) stat[i] = st;
@@ -334,6 +359,19 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
         }
     }
     s->active.swap(keep);
+    // 5. the jobs admitted during this step join their batches (from the
+    // next step on); jobs without sweeps are finished as they stand
+    for (auto& a : s->admitted) {
+        if (a.job.sweeps > 0 && sun_batch_add(s->batch_for(a.job), a.lat) != SUN_OK) {
+            sun_result r = blank_result(a.id, SUN_ERR_CUDA, a.submit_s);
+            sun_lattice_destroy(a.lat);
+            s->used -= a.bytes;
+            emit(r);
+            continue;
+        }
+        s->active.push_back(a);
+    }
+    s->admitted.clear();
     int done = 0;
     while (done < cap && !s->outbox.empty()) {
         out[done++] = s->outbox.front();

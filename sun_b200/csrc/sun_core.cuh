@@ -58,18 +58,45 @@ template <class R> struct PhiloxStream {
     }
     SUN_DEV R uniform();
 };
-template <> SUN_DEV float PhiloxStream<float>::uniform()
-{
-    uint32_t w = word();
-    return (float)((w >> 8) + 1u) * 5.9604644775390625e-08f;
-}
-template <> SUN_DEV double PhiloxStream<double>::uniform()
-{
-    uint32_t a = word();
-    uint32_t b = word();
-    uint64_t k = ((uint64_t)(a >> 11) << 32) | (uint64_t)b;
-    return (double)(k + 1ull) * 1.1102230246251565e-16;
-}
+// uniforms from a stream's words (FP32: one word, FP64: two)
+template <class R> struct WordsToUniform;
+template <> struct WordsToUniform<float> {
+    template <class S> static SUN_DEV float get(S& s)
+    {
+        uint32_t w = s.word();
+        return (float)((w >> 8) + 1u) * 5.9604644775390625e-08f;
+    }
+};
+template <> struct WordsToUniform<double> {
+    template <class S> static SUN_DEV double get(S& s)
+    {
+        uint32_t a = s.word();
+        uint32_t b = s.word();
+        uint64_t k = ((uint64_t)(a >> 11) << 32) | (uint64_t)b;
+        return (double)(k + 1ull) * 1.1102230246251565e-16;
+    }
+};
+template <class R> SUN_DEV R PhiloxStream<R>::uniform() { return WordsToUniform<R>::get(*this); }
+
+// The same stream with its first nb Philox blocks precomputed into shared
+// memory by other threads (words[b][j][lane]: word j of block b of the
+// stream of this lane's link).  The words, their order and the uniforms made
+// from them are those of PhiloxStream<R>; blocks past nb are computed here.
+template <class R> struct PrefetchedPhilox {
+    const uint32_t (*words)[4][32];
+    int nb, lane, n;
+    PhiloxStream<R> tail;  // its block counter starts at nb
+    SUN_DEV uint32_t word()
+    {
+        if (n < 4 * nb) {
+            const uint32_t v = words[n >> 2][n & 3][lane];
+            ++n;
+            return v;
+        }
+        return tail.word();
+    }
+    SUN_DEV R uniform() { return WordsToUniform<R>::get(*this); }
+};
 
 // Uniforms read from a caller buffer (oracle-parity mode); running out sets
 // an error flag and returns 0.5.

@@ -410,15 +410,40 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
 //
 // Shared memory (dynamic, tile_smem_bytes): B and D staging, N*N complex x
 // 32 sites each, then the staple sum S; U aliases the B/D staging once the
-// staples are summed.  Element e of a matrix sits at [e][lane]: a warp's
-// access to one element is 32 consecutive complex numbers (no bank
-// conflicts).
+// staples are summed; the heatbath adds the Philox words of its draws,
+// generated by all N warps before warp 0 runs the updates.  Element e of a
+// matrix sits at [e][lane]: a warp's access to one element is 32 consecutive
+// complex numbers (no bank conflicts).
 constexpr int kTileSites = 32;
-template <int N, class R> constexpr int tile_smem_bytes() { return 3 * N * N * kTileSites * (int)sizeof(cx<R>); }
+// Philox blocks of the heatbath prefetched per site: the words the N(N-1)/2
+// draws take when each accepts its first try (6 uniforms; FP64 2 words each)
+template <int N, class R> constexpr int tile_prefetch_blocks()
+{
+    return (N * (N - 1) / 2 * 6 * (int)(sizeof(R) / 4) + 3) / 4;
+}
+template <int N, class R, int MODE> constexpr int tile_smem_bytes()
+{
+    return 3 * N * N * kTileSites * (int)sizeof(cx<R>) +
+           (MODE == MODE_HB ? tile_prefetch_blocks<N, R>() * 4 * kTileSites * 4 : 0);
+}
+// CTAs per SM the tiled kernel's registers are capped for (FP32; 0: no cap,
+// the compiler's own choice; FP64 is uncapped).  More resident CTAs fill the
+// barrier waits while warp 0 of a CTA runs its SU(2) updates.  The heatbath,
+// which also holds the prefetch loop, would take 128 registers uncapped (2
+// CTAs of 192 threads per SM); capped for 3 CTAs it takes 96 without spills.
+#ifndef SUN_TILE_OCC_OR
+#define SUN_TILE_OCC_OR 0
+#endif
+#ifndef SUN_TILE_OCC_HB
+#define SUN_TILE_OCC_HB 3
+#endif
+template <class R, int MODE> struct TileOccupancy {
+    static constexpr int min_blocks = sizeof(R) == 4 ? (MODE == MODE_OR ? SUN_TILE_OCC_OR : SUN_TILE_OCC_HB) : 0;
+};
 
 template <int N, class R, int MODE>
-__global__ void __launch_bounds__(32 * N) k_update_tile(BatchView bv, int parity, int mu, unsigned hb_offset,
-                                                        InjView inj, int pdl)
+__global__ void __launch_bounds__(32 * N, (TileOccupancy<R, MODE>::min_blocks)) k_update_tile(
+    BatchView bv, int parity, int mu, unsigned hb_offset, InjView inj, int pdl)
 {
     static_assert(N >= 4, "the tiled update serves N >= 4");
     typedef cx<R> C;
@@ -427,6 +452,8 @@ __global__ void __launch_bounds__(32 * N) k_update_tile(BatchView bv, int parity
     C(*const Ds)[kTileSites] = Bs + N * N;
     C(*const Ss)[kTileSites] = Ds + N * N;
     C(*const Us)[kTileSites] = Bs;  // after the staple sum
+    // heatbath: the Philox words of the draws, [block][word][site]
+    uint32_t(*const Wd)[4][kTileSites] = reinterpret_cast<uint32_t(*)[4][kTileSites]>(Ss + N * N);
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;  // the row this warp owns
     const int b = blockIdx.x;
@@ -507,13 +534,33 @@ __global__ void __launch_bounds__(32 * N) k_update_tile(BatchView bv, int parity
         Ss[w * N + j][lane] = Sr[j];
         Us[w * N + j][lane] = ld_elem<R, LD_CG>(wbase + own + (uint32_t)(w * N + j) * stride);
     }
+    // heatbath: all N warps generate the Philox blocks warp 0's draws will
+    // read (the stream of PhiloxStream<R> for this site's link), so only
+    // rejected tries leave warp 0 computing blocks itself
+    constexpr int kPre = tile_prefetch_blocks<N, R>();
+    const uint32_t pass = MODE == MODE_HB ? L.state[0] + hb_offset : 0u;
+    if constexpr (MODE == MODE_HB) {
+        for (int bk = w; bk < kPre; bk += N) {
+            uint32_t c[4] = {(uint32_t)bk, (uint32_t)lex, (uint32_t)mu, pass};
+            philox4x32_10(c, (uint32_t)L.seed, (uint32_t)(L.seed >> 32));
+#pragma unroll
+            for (int q = 0; q < 4; ++q) Wd[bk][q][lane] = c[q];
+        }
+    }
     __syncthreads();
     if (w == 0) {
         // the subgroup sequence of overrelax_update / heatbath_update (N >= 4:
         // blocks of U S^dagger recomputed from U and S), rows from shared memory
-        PhiloxStream<R> ph;
+        PrefetchedPhilox<R> ph;
         InjectedStream<R> is;
-        if constexpr (MODE == MODE_HB) ph.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
+        if constexpr (MODE == MODE_HB) {
+            ph.words = Wd;
+            ph.nb = kPre;
+            ph.lane = lane;
+            ph.n = 0;
+            ph.tail.init(L.seed, (uint32_t)lex, (uint32_t)mu, pass);
+            ph.tail.blk = (uint32_t)kPre;
+        }
         if constexpr (MODE == MODE_HB_INJECTED) {
             is.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
             is.left = inj.stride;
@@ -1192,7 +1239,10 @@ template <int N, class R, int MODE> cudaError_t launch_tile(const BatchView& bv,
                                                             unsigned hb_offset, const InjView& inj, int pdl,
                                                             cudaStream_t s)
 {
-    constexpr int smem = tile_smem_bytes<N, R>();
+    constexpr int smem = tile_smem_bytes<N, R, MODE>();
+    // the dynamic size opted in above 48 KB.  The shared-memory carve-out is
+    // left to the driver: forcing the largest one measured slower (SU(6)
+    // 24^4 FP64 21.7 -> 38.0 ms per sweep, FP32 9.6 -> 10.7 ms).
     static const cudaError_t attr =
         smem > 48 * 1024
             ? cudaFuncSetAttribute(k_update_tile<N, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
