@@ -78,26 +78,6 @@ template <> struct WordsToUniform<double> {
 };
 template <class R> SUN_DEV R PhiloxStream<R>::uniform() { return WordsToUniform<R>::get(*this); }
 
-// The same stream with its first nb Philox blocks precomputed into shared
-// memory by other threads (words[b][j][lane]: word j of block b of the
-// stream of this lane's link).  The words, their order and the uniforms made
-// from them are those of PhiloxStream<R>; blocks past nb are computed here.
-template <class R> struct PrefetchedPhilox {
-    const uint32_t (*words)[4][32];
-    int nb, lane, n;
-    PhiloxStream<R> tail;  // its block counter starts at nb
-    SUN_DEV uint32_t word()
-    {
-        if (n < 4 * nb) {
-            const uint32_t v = words[n >> 2][n & 3][lane];
-            ++n;
-            return v;
-        }
-        return tail.word();
-    }
-    SUN_DEV R uniform() { return WordsToUniform<R>::get(*this); }
-};
-
 // Uniforms read from a caller buffer (oracle-parity mode); running out sets
 // an error flag and returns 0.5.
 template <class R> struct InjectedStream {

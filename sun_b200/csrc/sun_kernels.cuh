@@ -410,52 +410,46 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
 //
 // Shared memory (dynamic, tile_smem_bytes): B and D staging, N*N complex x
 // 32 sites each, then the staple sum S; U aliases the B/D staging once the
-// staples are summed; the heatbath adds the Philox words of its draws,
-// generated by all N warps before warp 0 runs the updates.  Element e of a
-// matrix sits at [e][lane]: a warp's access to one element is 32 consecutive
-// complex numbers (no bank conflicts).
+// staples are summed.  Element e of a matrix sits at [e][lane]: a warp's
+// access to one element is 32 consecutive complex numbers (no bank
+// conflicts).
 constexpr int kTileSites = 32;
-// Philox blocks of the heatbath prefetched per site: the words the N(N-1)/2
-// draws take when each accepts its first try (6 uniforms; FP64 2 words each)
-template <int N, class R> constexpr int tile_prefetch_blocks()
-{
-    return (N * (N - 1) / 2 * 6 * (int)(sizeof(R) / 4) + 3) / 4;
-}
-template <int N, class R, int MODE> constexpr int tile_smem_bytes()
-{
-    return 3 * N * N * kTileSites * (int)sizeof(cx<R>) +
-           (MODE == MODE_HB ? tile_prefetch_blocks<N, R>() * 4 * kTileSites * 4 : 0);
-}
+template <int N, class R> constexpr int tile_smem_bytes() { return 3 * N * N * kTileSites * (int)sizeof(cx<R>); }
 // CTAs per SM the tiled kernel's registers are capped for (FP32; 0: no cap,
-// the compiler's own choice; FP64 is uncapped).  More resident CTAs fill the
-// barrier waits while warp 0 of a CTA runs its SU(2) updates.  The heatbath,
-// which also holds the prefetch loop, would take 128 registers uncapped (2
-// CTAs of 192 threads per SM); capped for 3 CTAs it takes 96 without spills.
+// the compiler's own choice -- 72 registers for overrelaxation, 96 for the
+// heatbath; FP64 is uncapped).  Caps for 4 to 6 CTAs per SM measured no
+// faster (SU(6) 16^4, 24^4): other CTAs already fill the barrier waits while
+// warp 0 of a CTA runs its SU(2) updates, and the kernel is issue-bound.
 #ifndef SUN_TILE_OCC_OR
 #define SUN_TILE_OCC_OR 0
 #endif
 #ifndef SUN_TILE_OCC_HB
-#define SUN_TILE_OCC_HB 3
+#define SUN_TILE_OCC_HB 0
 #endif
 template <class R, int MODE> struct TileOccupancy {
     static constexpr int min_blocks = sizeof(R) == 4 ? (MODE == MODE_OR ? SUN_TILE_OCC_OR : SUN_TILE_OCC_HB) : 0;
 };
+// rows of the link matrices per warp (N / SUN_TILE_RPW warps per CTA): each
+// element staged in shared memory is read once for all of a warp's rows
+#ifndef SUN_TILE_RPW
+#define SUN_TILE_RPW 1
+#endif
+template <int N> constexpr int tile_rpw() { return N % SUN_TILE_RPW == 0 ? SUN_TILE_RPW : 1; }
 
 template <int N, class R, int MODE>
-__global__ void __launch_bounds__(32 * N, (TileOccupancy<R, MODE>::min_blocks)) k_update_tile(
+__global__ void __launch_bounds__(32 * N / tile_rpw<N>(), (TileOccupancy<R, MODE>::min_blocks)) k_update_tile(
     BatchView bv, int parity, int mu, unsigned hb_offset, InjView inj, int pdl)
 {
     static_assert(N >= 4, "the tiled update serves N >= 4");
+    constexpr int RW = tile_rpw<N>();  // rows w RW .. w RW + RW - 1 belong to warp w
     typedef cx<R> C;
     extern __shared__ __align__(16) unsigned char tile_raw[];
     C(*const Bs)[kTileSites] = reinterpret_cast<C(*)[kTileSites]>(tile_raw);
     C(*const Ds)[kTileSites] = Bs + N * N;
     C(*const Ss)[kTileSites] = Ds + N * N;
     C(*const Us)[kTileSites] = Bs;  // after the staple sum
-    // heatbath: the Philox words of the draws, [block][word][site]
-    uint32_t(*const Wd)[4][kTileSites] = reinterpret_cast<uint32_t(*)[4][kTileSites]>(Ss + N * N);
     const int lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;  // the row this warp owns
+    const int w = threadIdx.x >> 5;
     const int b = blockIdx.x;
     const int l = find_lat(bv, b);
     const LatDev& L = bv.lats[l];
@@ -481,9 +475,11 @@ __global__ void __launch_bounds__(32 * N, (TileOccupancy<R, MODE>::min_blocks)) 
     if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     auto Bget = [&](int k, int j) { return Bs[k * N + j][lane]; };
     auto Dget = [&](int k, int j) { return Ds[k * N + j][lane]; };
-    C Sr[N];
+    C Sr[RW][N];
 #pragma unroll
-    for (int j = 0; j < N; ++j) Sr[j] = mkc<R>(0, 0);
+    for (int r = 0; r < RW; ++r)
+#pragma unroll
+        for (int j = 0; j < N; ++j) Sr[r][j] = mkc<R>(0, 0);
     // the order over nu of k_update: rotated for N = 4, ascending for N = 6
     constexpr bool kRot = N <= 4;
 #pragma unroll 1
@@ -500,67 +496,56 @@ __global__ void __launch_bounds__(32 * N, (TileOccupancy<R, MODE>::min_blocks)) 
         const int syp = (lup >> 1) + other;                               // x + nu
         const int sy = (ldn >> 1) + other;                                // x - nu
         const int sz = (lex_step(ldn, xm, Xm, Sm, 1) >> 1) + parity * H;  // x - nu + mu
-        C a[N], c[N];
-        // up: row w of U_nu(x) U_mu(x+nu) U_nu(x+mu)^dagger
+        C a[RW][N], c[RW][N];
+        // up: rows i of U_nu(x) U_mu(x+nu) U_nu(x+mu)^dagger
 #pragma unroll
-        for (int k = 0; k < N; ++k) {
-            const uint32_t e = (uint32_t)(w * N + k) * stride;
-            a[k] = ld_elem<R, LD_CG>(base + (uint32_t)sx + nu * V + e);
-            Bs[w * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)syp + mu * V + e);
-            Ds[w * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sxpmu + nu * V + e);
-        }
-        __syncthreads();
-        rmul_g<N, R>(a, Bget, c);
-        racc_nd_g<N, R>(c, Dget, Sr);
-        __syncthreads();
-        // down: row w of U_nu(x-nu)^dagger U_mu(x-nu) U_nu(x-nu+mu)
+        for (int r = 0; r < RW; ++r)
 #pragma unroll
-        for (int k = 0; k < N; ++k) {
-            const uint32_t e = (uint32_t)(w * N + k) * stride;
-            a[k] = ld_elem<R, LD_CG>(base + (uint32_t)sy + nu * V + (uint32_t)(k * N + w) * stride);
-            Bs[w * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sy + mu * V + e);
-            Ds[w * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sz + nu * V + e);
-        }
+            for (int k = 0; k < N; ++k) {
+                const int i = w * RW + r;
+                const uint32_t e = (uint32_t)(i * N + k) * stride;
+                a[r][k] = ld_elem<R, LD_CG>(base + (uint32_t)sx + nu * V + e);
+                Bs[i * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)syp + mu * V + e);
+                Ds[i * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sxpmu + nu * V + e);
+            }
         __syncthreads();
-        rmul_dn_g<N, R>(a, Bget, c);
-        racc_g<N, R>(c, Dget, Sr);
+        rmul_rows_g<N, RW, R>(a, Bget, c);
+        racc_nd_rows_g<N, RW, R>(c, Dget, Sr);
+        __syncthreads();
+        // down: rows i of U_nu(x-nu)^dagger U_mu(x-nu) U_nu(x-nu+mu)
+#pragma unroll
+        for (int r = 0; r < RW; ++r)
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const int i = w * RW + r;
+                const uint32_t e = (uint32_t)(i * N + k) * stride;
+                a[r][k] = ld_elem<R, LD_CG>(base + (uint32_t)sy + nu * V + (uint32_t)(k * N + i) * stride);
+                Bs[i * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sy + mu * V + e);
+                Ds[i * N + k][lane] = ld_elem<R, LD_CG>(base + (uint32_t)sz + nu * V + e);
+            }
+        __syncthreads();
+        rmul_dn_rows_g<N, RW, R>(a, Bget, c);
+        racc_rows_g<N, RW, R>(c, Dget, Sr);
         __syncthreads();
     }
 
     cx<R>* wbase = reinterpret_cast<cx<R>*>(L.links);
     const uint32_t own = (uint32_t)sx + (uint32_t)mu * V;
 #pragma unroll
-    for (int j = 0; j < N; ++j) {
-        Ss[w * N + j][lane] = Sr[j];
-        Us[w * N + j][lane] = ld_elem<R, LD_CG>(wbase + own + (uint32_t)(w * N + j) * stride);
-    }
-    // heatbath: all N warps generate the Philox blocks warp 0's draws will
-    // read (the stream of PhiloxStream<R> for this site's link), so only
-    // rejected tries leave warp 0 computing blocks itself
-    constexpr int kPre = tile_prefetch_blocks<N, R>();
-    const uint32_t pass = MODE == MODE_HB ? L.state[0] + hb_offset : 0u;
-    if constexpr (MODE == MODE_HB) {
-        for (int bk = w; bk < kPre; bk += N) {
-            uint32_t c[4] = {(uint32_t)bk, (uint32_t)lex, (uint32_t)mu, pass};
-            philox4x32_10(c, (uint32_t)L.seed, (uint32_t)(L.seed >> 32));
+    for (int r = 0; r < RW; ++r)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) Wd[bk][q][lane] = c[q];
+        for (int j = 0; j < N; ++j) {
+            const int i = w * RW + r;
+            Ss[i * N + j][lane] = Sr[r][j];
+            Us[i * N + j][lane] = ld_elem<R, LD_CG>(wbase + own + (uint32_t)(i * N + j) * stride);
         }
-    }
     __syncthreads();
     if (w == 0) {
         // the subgroup sequence of overrelax_update / heatbath_update (N >= 4:
         // blocks of U S^dagger recomputed from U and S), rows from shared memory
-        PrefetchedPhilox<R> ph;
+        PhiloxStream<R> ph;
         InjectedStream<R> is;
-        if constexpr (MODE == MODE_HB) {
-            ph.words = Wd;
-            ph.nb = kPre;
-            ph.lane = lane;
-            ph.n = 0;
-            ph.tail.init(L.seed, (uint32_t)lex, (uint32_t)mu, pass);
-            ph.tail.blk = (uint32_t)kPre;
-        }
+        if constexpr (MODE == MODE_HB) ph.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
         if constexpr (MODE == MODE_HB_INJECTED) {
             is.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
             is.left = inj.stride;
@@ -610,7 +595,12 @@ __global__ void __launch_bounds__(32 * N, (TileOccupancy<R, MODE>::min_blocks)) 
     __syncthreads();
     if (valid) {
 #pragma unroll
-        for (int j = 0; j < N; ++j) st_elem<R>(wbase + own + (uint32_t)(w * N + j) * stride, Us[w * N + j][lane]);
+        for (int r = 0; r < RW; ++r)
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                const int i = w * RW + r;
+                st_elem<R>(wbase + own + (uint32_t)(i * N + j) * stride, Us[i * N + j][lane]);
+            }
     }
 }
 
@@ -1239,7 +1229,7 @@ template <int N, class R, int MODE> cudaError_t launch_tile(const BatchView& bv,
                                                             unsigned hb_offset, const InjView& inj, int pdl,
                                                             cudaStream_t s)
 {
-    constexpr int smem = tile_smem_bytes<N, R, MODE>();
+    constexpr int smem = tile_smem_bytes<N, R>();
     // the dynamic size opted in above 48 KB.  The shared-memory carve-out is
     // left to the driver: forcing the largest one measured slower (SU(6)
     // 24^4 FP64 21.7 -> 38.0 ms per sweep, FP32 9.6 -> 10.7 ms).
@@ -1248,7 +1238,7 @@ template <int N, class R, int MODE> cudaError_t launch_tile(const BatchView& bv,
             ? cudaFuncSetAttribute(k_update_tile<N, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
             : cudaSuccess;
     if (attr != cudaSuccess) return attr;
-    return launch_phase(k_update_tile<N, R, MODE>, bv, 32 * N, parity, mu, hb_offset, inj, pdl, s, smem);
+    return launch_phase(k_update_tile<N, R, MODE>, bv, 32 * N / tile_rpw<N>(), parity, mu, hb_offset, inj, pdl, s, smem);
 }
 
 template <int N>

@@ -288,6 +288,69 @@ template <int N, class R, class G> SUN_DEV void racc_g(const cx<R> a[N], G&& B, 
     }
 }
 
+// The same for RW rows at once: each element of B is read once for all RW
+// rows, and each row goes through exactly the operations above.
+template <int N, int RW, class R, class G> SUN_DEV void rmul_rows_g(const cx<R> (&a)[RW][N], G&& B, cx<R> (&c)[RW][N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        const cx<R> b0 = B(0, j);
+        cx<R> s[RW];
+#pragma unroll
+        for (int r = 0; r < RW; ++r) s[r] = a[r][0] * b0;
+#pragma unroll
+        for (int k = 1; k < N; ++k) {
+            const cx<R> bk = B(k, j);
+#pragma unroll
+            for (int r = 0; r < RW; ++r) s[r] = cfma(a[r][k], bk, s[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < RW; ++r) c[r][j] = s[r];
+    }
+}
+template <int N, int RW, class R, class G>
+SUN_DEV void rmul_dn_rows_g(const cx<R> (&a)[RW][N], G&& B, cx<R> (&c)[RW][N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> s[RW];
+#pragma unroll
+        for (int r = 0; r < RW; ++r) s[r] = mkc<R>(0, 0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const cx<R> bk = B(k, j);
+#pragma unroll
+            for (int r = 0; r < RW; ++r) s[r] = cfma_cn(a[r][k], bk, s[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < RW; ++r) c[r][j] = s[r];
+    }
+}
+template <int N, int RW, class R, class G>
+SUN_DEV void racc_nd_rows_g(const cx<R> (&a)[RW][N], G&& B, cx<R> (&s)[RW][N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const cx<R> bjk = B(j, k);
+#pragma unroll
+            for (int r = 0; r < RW; ++r) s[r][j] = cfma_nc(a[r][k], bjk, s[r][j]);
+        }
+}
+template <int N, int RW, class R, class G>
+SUN_DEV void racc_rows_g(const cx<R> (&a)[RW][N], G&& B, cx<R> (&s)[RW][N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j)
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const cx<R> bkj = B(k, j);
+#pragma unroll
+            for (int r = 0; r < RW; ++r) s[r][j] = cfma(a[r][k], bkj, s[r][j]);
+        }
+}
+
 // row 2 of an SU(3) matrix from rows 0, 1 -- rebuild12
 template <class R> SUN_DEV void rebuild12_row(const cx<R> a[3], const cx<R> b[3], cx<R> c[3])
 {

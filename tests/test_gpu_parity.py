@@ -470,8 +470,9 @@ def test_sweep_limit_stops_each_lattice_at_its_count(ctx):
     batch, alone, mixed = Batch(ctx), [], []
     for i, (d, limit, N, prec, lay) in enumerate([((4, 4, 4, 8), 3, 3, "f32", 1), ((6, 6, 6, 6), 5, 3, "f64", 0),
                                                    ((4, 4, 4, 4), 1, 4, "f32", 0), ((8, 8, 8, 8), 0, 3, "f32", 1),
-                                                   ((4, 4, 4, 4), 4, 2, "f32", 0)]):
-        beta = {2: 2.2, 3: 5.9, 4: 10.5}[N]
+                                                   ((4, 4, 4, 4), 4, 2, "f32", 0), ((4, 4, 4, 6), 2, 6, "f32", 0),
+                                                   ((4, 4, 4, 4), 0, 6, "f64", 0)]):
+        beta = {2: 2.2, 3: 5.9, 4: 10.5, 6: 25.0}[N]
         a = _make(ctx, N, d, prec, lay, seed=60 + i, beta=beta, reunit_every=2)
         b = _make(ctx, N, d, prec, lay, seed=60 + i, beta=beta, reunit_every=2)
         a.Init(hot=True)
