@@ -395,18 +395,20 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
 }
 
 // ---------------------------------------------------------------------------
-// Tiled update for N >= 4 (full links): a CTA of N warps advances 32
-// half-sites, one per lane.  Warp w owns row w: it loads row w (up staple) or
-// column w (down staple) of the first factor of each staple straight into
-// registers, and the CTA stages the other two factors once in shared memory
-// (warp w loads their row w), so every link element is read from L2 exactly
-// once and every load is a 32-lane coalesced one.  Each warp then forms row w
-// of the six staple products with the row routines of k_update_rows (same
-// operations, same order: the same bits as k_update) and keeps row w of the
-// staple sum in registers.  The SU(2) subgroup updates run in warp 0, one
-// lane per site, streaming rows p and q of U and S from shared memory, so no
-// thread ever holds an N x N matrix: SU(6) needs no spills at a modest
-// register count, where one thread per site spills kilobytes.
+// Tiled update for N >= 4 (full links): a CTA of N / RW warps advances 32
+// half-sites, one per lane, and warp w owns the RW rows i = w RW .. w RW +
+// RW - 1 (tile_rpw).  Per staple, a warp loads its rows (up staple) or
+// columns (down staple) of the first factor straight into registers, and the
+// CTA stages the other two factors once in shared memory (each warp loads its
+// rows of them), so every link element is read from L2 exactly once and every
+// load is a 32-lane coalesced one.  Each warp then forms its rows of the six
+// staple products with the row routines of k_update_rows (same operations,
+// same order: the same bits as k_update; one shared-memory read serves all
+// the warp's rows) and keeps its rows of the staple sum in registers.  The
+// SU(2) subgroup updates run in warp 0, one lane per site, streaming rows p
+// and q of U and S from shared memory, so no thread ever holds an N x N
+// matrix: SU(6) needs no spills at a modest register count, where one thread
+// per site spills kilobytes.
 //
 // Shared memory (dynamic, tile_smem_bytes): B and D staging, N*N complex x
 // 32 sites each, then the staple sum S; U aliases the B/D staging once the
@@ -429,19 +431,30 @@ template <int N, class R> constexpr int tile_smem_bytes() { return 3 * N * N * k
 template <class R, int MODE> struct TileOccupancy {
     static constexpr int min_blocks = sizeof(R) == 4 ? (MODE == MODE_OR ? SUN_TILE_OCC_OR : SUN_TILE_OCC_HB) : 0;
 };
-// rows of the link matrices per warp (N / SUN_TILE_RPW warps per CTA): each
-// element staged in shared memory is read once for all of a warp's rows
-#ifndef SUN_TILE_RPW
-#define SUN_TILE_RPW 1
+// Rows of the link matrices per warp (N / rows warps per CTA): each element
+// staged in shared memory is read once for all of a warp's rows, so more
+// rows per warp mean fewer shared-memory reads and fewer, fuller warps.
+// Measured on B200 (SU(6) sweeps, ms, 1 / 2 / 3 rows per warp): FP32 16^4
+// 2.01 / 1.71 / 1.95, 24^4 9.60 / 7.86 / 7.79; FP64 16^4 4.59 / 4.31 / 3.51,
+// 24^4 21.8 / 20.9 / 17.4.  All give the same bits.
+#ifndef SUN_TILE_RPW_F32
+#define SUN_TILE_RPW_F32 2
 #endif
-template <int N> constexpr int tile_rpw() { return N % SUN_TILE_RPW == 0 ? SUN_TILE_RPW : 1; }
+#ifndef SUN_TILE_RPW_F64
+#define SUN_TILE_RPW_F64 3
+#endif
+template <int N, class R> constexpr int tile_rpw()
+{
+    constexpr int r = sizeof(R) == 4 ? SUN_TILE_RPW_F32 : SUN_TILE_RPW_F64;
+    return N % r == 0 ? r : (N % 2 == 0 ? 2 : 1);
+}
 
 template <int N, class R, int MODE>
-__global__ void __launch_bounds__(32 * N / tile_rpw<N>(), (TileOccupancy<R, MODE>::min_blocks)) k_update_tile(
+__global__ void __launch_bounds__(32 * N / tile_rpw<N, R>(), (TileOccupancy<R, MODE>::min_blocks)) k_update_tile(
     BatchView bv, int parity, int mu, unsigned hb_offset, InjView inj, int pdl)
 {
     static_assert(N >= 4, "the tiled update serves N >= 4");
-    constexpr int RW = tile_rpw<N>();  // rows w RW .. w RW + RW - 1 belong to warp w
+    constexpr int RW = tile_rpw<N, R>();  // rows w RW .. w RW + RW - 1 belong to warp w
     typedef cx<R> C;
     extern __shared__ __align__(16) unsigned char tile_raw[];
     C(*const Bs)[kTileSites] = reinterpret_cast<C(*)[kTileSites]>(tile_raw);
@@ -1238,7 +1251,8 @@ template <int N, class R, int MODE> cudaError_t launch_tile(const BatchView& bv,
             ? cudaFuncSetAttribute(k_update_tile<N, R, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
             : cudaSuccess;
     if (attr != cudaSuccess) return attr;
-    return launch_phase(k_update_tile<N, R, MODE>, bv, 32 * N / tile_rpw<N>(), parity, mu, hb_offset, inj, pdl, s, smem);
+    return launch_phase(k_update_tile<N, R, MODE>, bv, 32 * N / tile_rpw<N, R>(), parity, mu, hb_offset, inj, pdl, s,
+                        smem);
 }
 
 template <int N>
