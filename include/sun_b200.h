@@ -88,6 +88,12 @@ const char *sun_version(void);
  * after_n more device allocations succeed, every further one reports
  * SUN_ERR_OUT_OF_MEMORY without calling the allocator; -1 turns it off */
 sun_status sun_debug_fail_allocations(int after_n);
+/* test hook of the resident sweeps (no reference counterpart): wait_ns
+ * bounds each grid barrier wait of k_sweeps_resident (<= 0: one second);
+ * skip_cta >= 0 makes that CTA leave at its first barrier without
+ * arriving, so the other CTAs' waits run out and sun_sweep_measure reports
+ * SUN_ERR_DEVICE_FLAG with the links part-updated (-1: off) */
+sun_status sun_debug_resident_barrier(sun_ctx *ctx, long long wait_ns, int skip_cta);
 
 /* ---- gauge arrays: _gauge<Real>(ArrayType, Device, 4V, evenodd) + Allocate
  * (include/gaugearray.h:139, :603) with SETPARAMS geometry
@@ -140,7 +146,12 @@ sun_status sun_sweep(sun_lattice *lat, int n_hb, int n_or, int n_sweeps, void *s
  * src/meas/polyakovloop.cu:637) in one call, with the same results as
  * sun_sweep + sun_plaquette + sun_polyakov per sweep.  plaq[2i], plaq[2i+1]:
  * spatial and temporal plaquette after sweep i; poly[2i], poly[2i+1]:
- * Polyakov loop; host arrays of 2 n_sweeps doubles, either may be NULL. */
+ * Polyakov loop; host arrays of 2 n_sweeps doubles, either may be NULL.
+ * A small SU(3) FP32 lattice (at most 16384 half-sites; SUN_B200_RESIDENT=
+ * 0|1|auto, SUN_B200_RESIDENT_MAX_HALFV) runs all n_sweeps in one
+ * cooperative launch whose grid barriers replace the launch boundaries,
+ * with the same results; a barrier wait that runs out (one second) returns
+ * SUN_ERR_DEVICE_FLAG. */
 sun_status sun_sweep_measure(sun_lattice *lat, int n_hb, int n_or, int n_sweeps, double *plaq, double *poly,
                              void *stream);
 /* one heatbath pass fed caller uniforms (oracle parity): device buffer

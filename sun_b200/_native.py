@@ -78,6 +78,7 @@ _SIGS = {
     "sun_unitarity_violation": [_vp, _dp, _vp],
     "sun_link_trace_det": [_vp, _dp, _vp],
     "sun_debug_fail_allocations": [C.c_int],
+    "sun_debug_resident_barrier": [C.c_void_p, C.c_longlong, C.c_int],
     "sun_debug_su2_draws": [C.c_int, C.c_double, C.c_uint64, C.c_int, _dp],
     "sun_plaquette": [_vp, _dp, _vp],
     "sun_plaquette_noalloc": [_vp, C.POINTER(SunLatticeParams), _vp, _vp],

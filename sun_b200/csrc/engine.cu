@@ -143,6 +143,20 @@ struct sun_ctx {
     // (SUN_B200_PDL=0 turns it off)
     int pdl = 1;
     long long rows_max_halfv = 16384;
+    // sun_sweep_measure in one cooperative launch (k_sweeps_resident): -1
+    // for SU(3) FP32 lattices of at most resident_max_halfv half-sites, 0
+    // never, 1 whenever the lattice and launch shapes allow
+    // (SUN_B200_RESIDENT).  Measured on B200, 1 HB + 4 OR with both
+    // observables per sweep, us per sweep resident / captured graph: SU(3)
+    // FP32 8^4 189 / 206 (full links), 191 / 195 (12-parameter), 12^4
+    // 207 / 233; slower for FP64 (SU(3) 8^4 232 / 200, 12^4 297 / 268),
+    // SU(2) (8^4 131 / 111), SU(4) (8^4 271 / 224) and from 16^4 up.
+    int resident = -1;
+    long long resident_max_halfv = 16384;
+    unsigned long long barrier_wait_ns = 1000000000ull;  // one grid barrier wait at most
+    int skip_arrive = -1;  // test hook (sun_debug_resident_barrier)
+    DevBuf res_sync;       // barrier count, generation, status
+    DevBuf res_out;        // per-sweep plaquette and Polyakov sums
     // autotuner (tuneLaunch, src/tune.cpp:304): CTA size of the update kernel
     // per (kernel class, total half-volume), timed once, cached in a CSV file
     bool tune = false;
@@ -174,7 +188,10 @@ struct sun_lattice {
     int meas_hb = -1, meas_or = -1;
     unsigned meas_version = 0;
     size_t meas_rows = 0;
-    DevBuf meas, slot;
+    // meas_part: the captured measurements' CTA partials, owned by the graph
+    // (a shared scratch buffer could be reallocated under it by a later
+    // call that needs more partials)
+    DevBuf meas, slot, meas_part;
     ~sun_lattice();
 };
 
@@ -687,6 +704,15 @@ sun_status sun_debug_fail_allocations(int after_n)
     return SUN_OK;
 }
 
+sun_status sun_debug_resident_barrier(sun_ctx* c, long long wait_ns, int skip_cta)
+{
+    if (!c) return SUN_ERR_INVALID_ARG;
+    return handle(c, [&] {
+        c->barrier_wait_ns = wait_ns > 0 ? (unsigned long long)wait_ns : 1000000000ull;
+        c->skip_arrive = skip_cta < 0 ? -1 : skip_cta;
+    });
+}
+
 const char* sun_last_error_string(const sun_ctx* c)
 {
     if (c) return c->last_error.c_str();
@@ -749,6 +775,8 @@ sun_status sun_init(const sun_config* cfg, sun_ctx** out)
             else if (!strcmp(k, "tile")) c->upd_kernel = 3;
         }
         if (const char* t = getenv("SUN_B200_ROWS_MAX_HALFV")) c->rows_max_halfv = atoll(t);
+        if (const char* t = getenv("SUN_B200_RESIDENT")) c->resident = !strcmp(t, "auto") ? -1 : (atoi(t) ? 1 : 0);
+        if (const char* t = getenv("SUN_B200_RESIDENT_MAX_HALFV")) c->resident_max_halfv = atoll(t);
         if (const char* t = getenv("SUN_B200_PDL")) c->pdl = atoi(t) ? 1 : 0;
         *out = c.release();
     });
@@ -1094,14 +1122,14 @@ static bool solo_measure_graph(sun_lattice* l, Group& g, int n_hb, int n_or, siz
     if (n_or > 0) upd_view(g, update_block(c, g, MODE_OR, s), s);
     if (re) g.view(WORK_LINKS, c->blk_links, s);
     BatchView vp = g.view(WORK_PLANES, c->blk_sites, s), vl = g.view(WORK_POLY8, c->blk_sites, s);
-    g.partials.ensure(sizeof(double) * 4 * (size_t)std::max(1, std::max(vp.nblocks, vl.nblocks)));
+    l->meas_part.ensure(sizeof(double) * 4 * (size_t)std::max(1, std::max(vp.nblocks, vl.nblocks)));
     if (g.counters_n < g.lats.size()) {
         g.counters.ensure(sizeof(unsigned) * g.lats.size());
         ck(cudaMemsetAsync(g.counters.p, 0, sizeof(unsigned) * g.lats.size(), s), "counters");
         g.counters_n = g.lats.size();
     }
     ck(cudaStreamSynchronize(s), "measure graph setup");
-    double* part = reinterpret_cast<double*>(g.partials.p);
+    double* part = reinterpret_cast<double*>(l->meas_part.p);
     unsigned* cnt = reinterpret_cast<unsigned*>(g.counters.p);
     unsigned* slot = reinterpret_cast<unsigned*>(l->slot.p);
     double* out_p = reinterpret_cast<double*>(l->meas.p);
@@ -1132,6 +1160,74 @@ static bool solo_measure_graph(sun_lattice* l, Group& g, int n_hb, int n_or, siz
     return true;
 }
 
+// sun_sweep_measure as one cooperative launch (k_sweeps_resident), for a
+// lattice whose launched phases are latency-bound.  Returns false, having
+// launched nothing, when the lattice, the launch shapes or the stream do not
+// allow it.
+static bool resident_sweeps(sun_lattice* l, Group& g, int n_hb, int n_or, int n_sweeps, double* plaq, double* poly,
+                            cudaStream_t s)
+{
+    sun_ctx* c = l->ctx;
+    const LatDev& L = l->desc;
+    if (c->resident == 0 || L.sweep_limit != 0u || c->blk_sites != 128 || g.N > 4) return false;
+    if (c->resident < 0 && (g.N != 3 || g.fp64 || L.halfV > c->resident_max_halfv)) return false;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return false;
+    // the launched path's update shapes: one thread per half-site or the
+    // row-split kernel, CTAs of 128 threads, the same for both modes
+    const int cfg_hb = n_hb > 0 ? update_block(c, g, MODE_HB, s) : 0;
+    const int cfg_or = n_or > 0 ? update_block(c, g, MODE_OR, s) : 0;
+    const int cfg = n_hb > 0 ? cfg_hb : cfg_or;
+    if ((n_hb > 0 && n_or > 0 && cfg_hb != cfg_or) || (cfg != 128 && cfg != -128)) return false;
+    const int rows = cfg < 0;
+    int cap_ctas = 0;
+    switch (g.N) {
+    case 2: cap_ctas = Ops<2>::resident_capacity(g.fp64, g.layout, rows); break;
+    case 3: cap_ctas = Ops<3>::resident_capacity(g.fp64, g.layout, rows); break;
+    case 4: cap_ctas = Ops<4>::resident_capacity(g.fp64, g.layout, rows); break;
+    default: break;
+    }
+    if (cap_ctas < 2) return false;
+    BatchView upd = upd_view(g, cfg, s);
+    BatchView vp = g.view(WORK_PLANES, 128, s), vl = g.view(WORK_POLY8, 128, s);
+    g.partials.ensure(sizeof(double) * 4 * (size_t)(vp.nblocks + vl.nblocks));
+    c->res_sync.ensure(4 * sizeof(unsigned));
+    c->res_out.ensure(sizeof(double) * 4 * (size_t)n_sweeps);
+    ck(cudaMemsetAsync(c->res_sync.p, 0, 4 * sizeof(unsigned), s), "barrier reset");
+    ResidentArgs a{};
+    a.upd = upd;
+    a.plaq = vp;
+    a.poly = vl;
+    a.n_hb = n_hb;
+    a.n_or = n_or;
+    a.n_sweeps = n_sweeps;
+    a.partials = reinterpret_cast<double*>(g.partials.p);
+    a.out_plaq = reinterpret_cast<double*>(c->res_out.p);
+    a.out_poly = a.out_plaq + 2 * (size_t)n_sweeps;
+    a.bar = reinterpret_cast<unsigned*>(c->res_sync.p);
+    a.status = reinterpret_cast<int*>(a.bar + 2);
+    a.wait_ns = c->barrier_wait_ns;
+    a.skip_arrive = c->skip_arrive;
+    // two sets of CTAs that take the phases in turn, each covering the
+    // update's CTAs (several per resident CTA when they do not all fit)
+    const int grid = 2 * std::max(1, std::min(cap_ctas / 2, upd.nblocks));
+    OPS_CALL(g.N, sweeps_resident, g.fp64, g.layout, rows, a, grid, s);
+    std::vector<double> h(4 * (size_t)n_sweeps);
+    int status = 0;
+    ck(cudaMemcpyAsync(h.data(), c->res_out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s), "copy");
+    ck(cudaMemcpyAsync(&status, a.status, sizeof(int), cudaMemcpyDeviceToHost, s), "status copy");
+    ck(cudaStreamSynchronize(s), "resident sweeps");
+    if (status)
+        fail(SUN_ERR_DEVICE_FLAG, "a grid barrier wait of the resident sweeps ran out (limit %llu ns); the links "
+             "are left part-updated", (unsigned long long)c->barrier_wait_ns);
+    const double np = 3.0 * l->p.ncolors * (double)L.V, nl = (double)l->p.ncolors * L.X[0] * L.X[1] * L.X[2];
+    for (int i = 0; i < 2 * n_sweeps; ++i) {
+        if (plaq) plaq[i] = h[i] / np;
+        if (poly) poly[i] = h[2 * (size_t)n_sweeps + i] / nl;
+    }
+    return true;
+}
+
 sun_status sun_sweep_measure(sun_lattice* l, int n_hb, int n_or, int n_sweeps, double* plaq, double* poly,
                              void* stream)
 {
@@ -1141,6 +1237,7 @@ sun_status sun_sweep_measure(sun_lattice* l, int n_hb, int n_or, int n_sweeps, d
         cudaStream_t s = S(l->ctx, stream);
         if (n_sweeps == 0) return;
         Solo so(l);
+        if (resident_sweeps(l, so.g, n_hb, n_or, n_sweeps, plaq, poly, s)) return;
         if (solo_measure_graph(l, so.g, n_hb, n_or, (size_t)n_sweeps, s)) {
             // n replays back to back, one copy of the observables at the end;
             // normalised on the host as sun_plaquette / sun_polyakov do

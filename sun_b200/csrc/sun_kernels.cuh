@@ -89,14 +89,36 @@ template <class R, int MODE, int LAYOUT> struct UpdateOccupancy<3, R, MODE, LAYO
 };
 
 // ---------------------------------------------------------------------------
+// Where an update waits for the phase before it.  That phase wrote the links
+// of direction dep = mu - 1 (mod 4), which only the staples of nu = dep
+// read: the staples before it are summed while the previous phase drains,
+// and the update waits (Dep::wait) just before the staple of nu = dep.
+// GdcDep: a launch that may be a programmatic dependent of the previous
+// phase (pdl != 0).  griddepcontrol.wait waits for that launch to complete,
+// and only after it the next phase may launch (launch_dependents), so a
+// launch never runs beside the one two back.  The resident sweeps wait on
+// their grid's arrival count instead (ResidentDep).
+struct GdcDep {
+    int pdl;
+    SUN_DEV int dep(int mu) const { return pdl ? ((mu + 3) & 3) : -1; }
+    SUN_DEV void start(int dep) const
+    {
+        if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    }
+    SUN_DEV void wait() const
+    {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    }
+};
+
 // One link update of the checkerboard phase (parity, mu): half-site id of
 // lattice L.  ld(i, e) returns element e of the link at image index i
-// (complex element i + 4 V e) and st(i, e, v) writes it.  GDC: the launch
-// may be a programmatic dependent of the previous phase (pdl != 0 then waits
-// for it before the staples of the direction that phase wrote).
-template <int N, class R, int LAYOUT, int MODE, bool GDC, class Ld, class St>
+// (complex element i + 4 V e) and st(i, e, v) writes it; dp: where and how
+// to wait for the previous phase.
+template <int N, class R, int LAYOUT, int MODE, class Dep, class Ld, class St>
 SUN_DEV void update_site(const Geom& g, const LatDev& L, int id, int parity, int mu, unsigned hb_offset,
-                         const InjView& inj, int pdl, Ld&& ld, St&& st)
+                         const InjView& inj, const Dep& dp, Ld&& ld, St&& st)
 {
     typedef LinkIO<N, R, LAYOUT> IO;
     const uint32_t V = (uint32_t)g.V, stride = 4u * V;
@@ -115,16 +137,8 @@ SUN_DEV void update_site(const Geom& g, const LatDev& L, int id, int parity, int
     const int other = (1 - parity) * H;
     const int sxpmu = (lex_step(lex, xm, Xm, Sm, 1) >> 1) + other;
 
-    // launched as a programmatic dependent of the previous phase (pdl): that
-    // phase wrote the links of direction dep = mu - 1 (mod 4), which only
-    // the staples of nu = dep read.  The staples before it are summed while
-    // the previous launch drains; griddepcontrol.wait then waits for it to
-    // complete, and only after that the next phase may launch (so a launch
-    // never runs beside the one two back).
-    const int dep = (GDC && pdl) ? ((mu + 3) & 3) : -1;
-    if constexpr (GDC) {
-        if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    }
+    const int dep = dp.dep(mu);
+    dp.start(dep);
     Mat<N, R> S;
     mzero(S);
     // N <= 4: nu = mu+1, mu+2, mu+3 (mod 4), the staple of the previous
@@ -136,10 +150,7 @@ SUN_DEV void update_site(const Geom& g, const LatDev& L, int id, int parity, int
     for (int kk = kRot ? 1 : 0; kk < 4; ++kk) {
         const int nu = kRot ? ((mu + kk) & 3) : kk;
         if (!kRot && nu == mu) continue;
-        if (GDC && nu == dep) {
-            asm volatile("griddepcontrol.wait;" ::: "memory");
-            asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-        }
+        if (nu == dep) dp.wait();
         const int xn_ = kRot ? sel4(x, nu) : x[kk], Xn_ = kRot ? sel4(g.X, nu) : g.X[kk],
                   Sn_ = kRot ? sel4(st_, nu) : st_[kk];
         const int lup = lex_step(lex, xn_, Xn_, Sn_, 1);
@@ -224,8 +235,8 @@ __global__ void __launch_bounds__(128, (UpdateOccupancy<N, R, MODE, LAYOUT>::min
     if (id >= g.halfV || lat_frozen(L)) return;
     cx<R>* base = reinterpret_cast<cx<R>*>(L.links);
     const uint32_t stride = 4u * (uint32_t)g.V;
-    update_site<N, R, LAYOUT, MODE, true>(
-        g, L, id, parity, mu, hb_offset, inj, pdl,
+    update_site<N, R, LAYOUT, MODE>(
+        g, L, id, parity, mu, hb_offset, inj, GdcDep{pdl},
         [&](uint32_t i, int e) { return ld_elem<R, LD_CG>(base + i + e * stride); },
         [&](uint32_t i, int e, cx<R> v) { st_elem<R>(base + i + e * stride, v); });
 }
@@ -246,9 +257,11 @@ template <class R> SUN_DEV cx<R> shfl_cx(cx<R> v, int src)
 // goes through the same operations in the same order as in k_update (the row
 // routines of sun_math.cuh), so both kernels give the same bits and either
 // may run any lattice.
-template <int N, class R, int LAYOUT, int MODE>
-__global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, int mu, unsigned hb_offset,
-                                                     InjView inj, int pdl)
+// The row-split update of the warp whose first half-site is `first` (<
+// halfV); dp as in update_site.
+template <int N, class R, int LAYOUT, int MODE, class Dep>
+SUN_DEV void update_rows_warp(const Geom& g, const LatDev& L, int first, int parity, int mu, unsigned hb_offset,
+                              const InjView& inj, const Dep& dp)
 {
     constexpr int SPW = 32 / N;  // sites per warp; lanes 32 - 32 % N .. 31 shadow the last site
     const int lane = threadIdx.x & 31;
@@ -257,12 +270,6 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
     const int slot = used ? grp : SPW - 1;
     const int r = used ? lane - grp * N : lane % N;
     const int lead = slot * N;  // the lane holding row 0 of this site
-    const int b = blockIdx.x;
-    const int l = find_lat(bv, b);
-    const LatDev& L = bv.lats[l];
-    const Geom g = geom_of(L);
-    const int first = (b - __ldg(bv.begin + l)) * ((int)(blockDim.x >> 5) * SPW) + (int)(threadIdx.x >> 5) * SPW;
-    if (first >= g.halfV || lat_frozen(L)) return;  // the whole warp is past the end, or the lattice done
     const int id0 = first + slot;
     const bool valid = used && id0 < g.halfV;
     const int id = id0 < g.halfV ? id0 : g.halfV - 1;  // past the end: compute a copy, store nothing
@@ -282,8 +289,8 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
     const int other = (1 - parity) * H;
     const int sxpmu = (lex_step(lex, xm, Xm, Sm, 1) >> 1) + other;
 
-    const int dep = pdl ? ((mu + 3) & 3) : -1;  // as in k_update
-    if (dep < 0) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int dep = dp.dep(mu);
+    dp.start(dep);
     cx<R> Sr[N];  // row r of the staple sum
 #pragma unroll
     for (int j = 0; j < N; ++j) Sr[j] = mkc<R>(0, 0);
@@ -296,10 +303,7 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
     for (int kk = kRot ? 1 : 0; kk < 4; ++kk) {
         const int nu = kRot ? ((mu + kk) & 3) : kk;
         if (!kRot && nu == mu) continue;
-        if (nu == dep) {
-            asm volatile("griddepcontrol.wait;" ::: "memory");
-            asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-        }
+        if (nu == dep) dp.wait();
         const int xn_ = kRot ? sel4(x, nu) : x[kk], Xn_ = kRot ? sel4(g.X, nu) : g.X[kk],
                   Sn_ = kRot ? sel4(st, nu) : st[kk];
         const int lup = lex_step(lex, xn_, Xn_, Sn_, 1);
@@ -392,6 +396,20 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
         }
     }
     if (valid && r == 0) IO::store(wbase, own, stride, U);
+}
+
+template <int N, class R, int LAYOUT, int MODE>
+__global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, int mu, unsigned hb_offset,
+                                                     InjView inj, int pdl)
+{
+    constexpr int SPW = 32 / N;
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int first = (b - __ldg(bv.begin + l)) * ((int)(blockDim.x >> 5) * SPW) + (int)(threadIdx.x >> 5) * SPW;
+    if (first >= g.halfV || lat_frozen(L)) return;  // the whole warp is past the end, or the lattice done
+    update_rows_warp<N, R, LAYOUT, MODE>(g, L, first, parity, mu, hb_offset, inj, GdcDep{pdl});
 }
 
 // ---------------------------------------------------------------------------
@@ -708,7 +726,19 @@ __global__ void __launch_bounds__(128) k_hot(BatchView bv)
 }
 
 // FP64 reunitarization of every link -- kernel_calc_reunitarize
-// (src/reunitarize.cu:23-31), always in double arithmetic.
+// (src/reunitarize.cu:23-31), always in double arithmetic.  Link w (image
+// index) of lattice L, loaded through path P.
+template <int N, class R, int LAYOUT, int P> SUN_DEV void reunit_link(const LatDev& L, int w)
+{
+    cx<R>* base = reinterpret_cast<cx<R>*>(L.links);
+    Mat<N, R> U;
+    LinkIO<N, R, LAYOUT>::template load<P>(base, (uint32_t)w, 4u * L.V, U);
+    Mat<N, double> D;
+    mconvert(U, D);
+    reunit<N, double>(D);
+    mconvert(D, U);
+    LinkIO<N, R, LAYOUT>::store(base, (uint32_t)w, 4u * L.V, U);
+}
 template <int N, class R, int LAYOUT>
 __global__ void __launch_bounds__(256) k_reunit(BatchView bv, int only_due)
 {
@@ -724,14 +754,7 @@ __global__ void __launch_bounds__(256) k_reunit(BatchView bv, int only_due)
     }
     const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
     if (w >= 4 * L.V) return;
-    cx<R>* base = reinterpret_cast<cx<R>*>(L.links);
-    Mat<N, R> U;
-    LinkIO<N, R, LAYOUT>::template load<false>(base, (uint32_t)w, 4u * L.V, U);
-    Mat<N, double> D;
-    mconvert(U, D);
-    reunit<N, double>(D);
-    mconvert(D, U);
-    LinkIO<N, R, LAYOUT>::store(base, (uint32_t)w, 4u * L.V, U);
+    reunit_link<N, R, LAYOUT, LD_CA>(L, w);
 }
 
 // ---------------------------------------------------------------------------
@@ -783,6 +806,25 @@ SUN_DEV void block_sum(double v, double* out, DD* sh)
 // out (host-mapped memory allowed); the counter is left at zero.  slot (may
 // be null): a device counter; the results go to row *slot of out (nlat *
 // nvals doubles per row), so a replayed graph fills one row per replay.
+// The sums of CTA partials b0 .. b1 - 1 (nvals values each), by one warp
+// (lane = threadIdx.x < 32): lane-strided compensated sums, then the shuffle
+// tree; lane 0 writes value v to dst[v].
+SUN_DEV void finalize_partials(const double* partials, int b0, int b1, int nvals, double* dst)
+{
+    const int lane = threadIdx.x;
+    for (int v = 0; v < nvals; ++v) {
+        DD d;
+        d.s = 0.0; d.c = 0.0;
+        for (int b = b0 + lane; b < b1; b += 32) {
+            DD t;
+            t.s = __ldcg(partials + ((size_t)b * nvals + v) * 2);
+            t.c = __ldcg(partials + ((size_t)b * nvals + v) * 2 + 1);
+            d = dd_add(d, t);
+        }
+        d = dd_warp(d);
+        if (lane == 0) dst[v] = d.s + d.c;
+    }
+}
 SUN_DEV void finalize_if_last(const BatchView& bv, int l, const double* partials, int nvals, double* out,
                               unsigned* counters, const unsigned* slot)
 {
@@ -796,22 +838,9 @@ SUN_DEV void finalize_if_last(const BatchView& bv, int l, const double* partials
     __syncthreads();
     if (!last || threadIdx.x >= 32) return;
     __threadfence();
-    const int lane = threadIdx.x;
-    const int b0 = __ldg(bv.begin + l), b1 = __ldg(bv.begin + l + 1);
-    for (int v = 0; v < nvals; ++v) {
-        DD d;
-        d.s = 0.0; d.c = 0.0;
-        for (int b = b0 + lane; b < b1; b += 32) {
-            DD t;
-            t.s = __ldcg(partials + ((size_t)b * nvals + v) * 2);
-            t.c = __ldcg(partials + ((size_t)b * nvals + v) * 2 + 1);
-            d = dd_add(d, t);
-        }
-        d = dd_warp(d);
-        const size_t row = slot ? (size_t)__ldcg(slot) * (size_t)bv.nlat * nvals : 0;
-        if (lane == 0) out[row + (size_t)l * nvals + v] = d.s + d.c;
-    }
-    if (lane == 0) counters[l] = 0u;
+    const size_t row = slot ? (size_t)__ldcg(slot) * (size_t)bv.nlat * nvals : 0;
+    finalize_partials(partials, __ldg(bv.begin + l), __ldg(bv.begin + l + 1), nvals, out + row + (size_t)l * nvals);
+    if (threadIdx.x == 0) counters[l] = 0u;
 }
 
 SUN_DEV void block_max(double v, double* out, double* sh)
@@ -845,11 +874,11 @@ SUN_DEV int site_index(const LatDev& L, const Geom& g, const int x[4])
     return L.evenodd ? eo_of(g, x) : lex_of(g, x);
 }
 
-template <int N, class R, int LAYOUT>
+template <int N, class R, int LAYOUT, int P = LD_NC>
 SUN_DEV void load_d(const LatDev& L, const Geom& g, const int x[4], int mu, Mat<N, double>& D)
 {
     Mat<N, R> A;
-    LinkIO<N, R, LAYOUT>::template load<true>(reinterpret_cast<const cx<R>*>(L.links),
+    LinkIO<N, R, LAYOUT>::template load<P>(reinterpret_cast<const cx<R>*>(L.links),
                                               (uint32_t)site_index(L, g, x) + (uint32_t)mu * g.V,
                                               4u * g.V, A);
     mconvert(A, D);
@@ -866,20 +895,51 @@ SUN_DEV void load_d(const LatDev& L, const Geom& g, const int x[4], int mu, Mat<
 // order whatever the storage order, so the neighbours x + mu, x + nu that a
 // CTA reads are read by the CTAs beside it at about the same time (walking
 // one even/odd block after the other fetched every link from DRAM twice).
-template <int N, class R, int LAYOUT>
+template <int N, class R, int LAYOUT, int LP = LD_NC>
 SUN_DEV double plaquette_plane(const LatDev& L, const Geom& g, const int x[4], int mu, int nu)
 {
     int xm[4], xn[4];
     shifted(g, x, mu, 1, xm);
     shifted(g, x, nu, 1, xn);
     Mat<N, double> A, B, P, Q;
-    load_d<N, R, LAYOUT>(L, g, x, mu, A);
-    load_d<N, R, LAYOUT>(L, g, xm, nu, B);
+    load_d<N, R, LAYOUT, LP>(L, g, x, mu, A);
+    load_d<N, R, LAYOUT, LP>(L, g, xm, nu, B);
     mmul(A, B, P);
-    load_d<N, R, LAYOUT>(L, g, x, nu, A);
-    load_d<N, R, LAYOUT>(L, g, xn, mu, B);
+    load_d<N, R, LAYOUT, LP>(L, g, x, nu, A);
+    load_d<N, R, LAYOUT, LP>(L, g, xn, mu, B);
     mmul(A, B, Q);
     return mtrace_nd(P, Q).re;
+}
+
+// plaquette work item w of lattice L (thread w of k_plaquette's CTAs over
+// the lattice): its spatial and temporal sums, links loaded through path P
+template <int N, class R, int LAYOUT, int P>
+SUN_DEV void plaquette_item(const LatDev& L, const Geom& g, int w, double& sp, double& tp)
+{
+    sp = 0.0;
+    tp = 0.0;
+    if (g.V < kPlaneSplitMaxV) {
+        const int chunk = w / 192, r = w - 192 * chunk, plane = r >> 5;
+        const int site = chunk * 32 + (r & 31);
+        if (site < g.V) {
+            const int mu = plane < 3 ? 0 : (plane < 5 ? 1 : 2);
+            const int nu = plane < 3 ? plane + 1 : (plane < 5 ? plane - 1 : 3);
+            int x[4];
+            lex_coords(g, site, x);
+            const double t = plaquette_plane<N, R, LAYOUT, P>(L, g, x, mu, nu);
+            if (nu == 3) tp = t; else sp = t;
+        }
+    } else if (w < g.V) {
+        int x[4];
+        lex_coords(g, w, x);
+#pragma unroll 1
+        for (int mu = 0; mu < 3; ++mu)
+#pragma unroll 1
+            for (int nu = mu + 1; nu < 4; ++nu) {
+                const double t = plaquette_plane<N, R, LAYOUT, P>(L, g, x, mu, nu);
+                if (nu == 3) tp += t; else sp += t;
+            }
+    }
 }
 
 template <int N, class R, int LAYOUT>
@@ -892,29 +952,8 @@ __global__ void __launch_bounds__(128) k_plaquette(BatchView bv, double* partial
     const LatDev& L = bv.lats[l];
     const Geom g = geom_of(L);
     const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
-    double sp = 0.0, tp = 0.0;
-    if (g.V < kPlaneSplitMaxV) {
-        const int chunk = w / 192, r = w - 192 * chunk, plane = r >> 5;
-        const int site = chunk * 32 + (r & 31);
-        if (site < g.V) {
-            const int mu = plane < 3 ? 0 : (plane < 5 ? 1 : 2);
-            const int nu = plane < 3 ? plane + 1 : (plane < 5 ? plane - 1 : 3);
-            int x[4];
-            lex_coords(g, site, x);
-            const double t = plaquette_plane<N, R, LAYOUT>(L, g, x, mu, nu);
-            if (nu == 3) tp = t; else sp = t;
-        }
-    } else if (w < g.V) {
-        int x[4];
-        lex_coords(g, w, x);
-#pragma unroll 1
-        for (int mu = 0; mu < 3; ++mu)
-#pragma unroll 1
-            for (int nu = mu + 1; nu < 4; ++nu) {
-                const double t = plaquette_plane<N, R, LAYOUT>(L, g, x, mu, nu);
-                if (nu == 3) tp += t; else sp += t;
-            }
-    }
+    double sp, tp;
+    plaquette_item<N, R, LAYOUT, LD_NC>(L, g, w, sp, tp);
     block_sum(sp, partials + (size_t)b * 4, sh);
     block_sum(tp, partials + (size_t)b * 4 + 2, sh);
     if (out) finalize_if_last(bv, l, partials, 2, out, counters, slot);
@@ -936,21 +975,17 @@ template <int N> SUN_DEV void shfl_mat(Mat<N, double>& D, const Mat<N, double>& 
 // (an empty range gives the unit matrix), then the lane products are joined
 // in order by a shuffle tree, (P0 P1)(P2 P3)..., so the time chain is T / 8
 // products plus three joins instead of T products.
-template <int N, class R, int LAYOUT>
-__global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials, double* out, unsigned* counters,
-                                                   const unsigned* slot)
+// Polyakov work item w of lattice L (thread w of k_polyakov's CTAs; all
+// lanes of the warp take part): the trace at the site of lane k == 0, links
+// loaded through path P
+template <int N, class R, int LAYOUT, int P>
+SUN_DEV void polyakov_item(const LatDev& L, const Geom& g, int w, double& re, double& im)
 {
-    __shared__ DD sh[32];
-    const int b = blockIdx.x;
-    const int l = find_lat(bv, b);
-    const LatDev& L = bv.lats[l];
-    const Geom g = geom_of(L);
     const int V3 = g.X[0] * g.X[1] * g.X[2];
-    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
     const int site = w / kPolyLanes, k = w - kPolyLanes * site;
     const bool valid = site < V3;
-    Mat<N, double> P, A, T;
-    munit(P);
+    Mat<N, double> Pm, A, T;
+    munit(Pm);
     if (valid) {
         int x[4];
         x[0] = site % g.X[0];
@@ -960,9 +995,9 @@ __global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials
 #pragma unroll 1
         for (int t = t0; t < t1; ++t) {
             x[3] = t;
-            load_d<N, R, LAYOUT>(L, g, x, 3, A);
-            mmul(P, A, T);
-            P = T;
+            load_d<N, R, LAYOUT, P>(L, g, x, 3, A);
+            mmul(Pm, A, T);
+            Pm = T;
         }
     }
     // blockDim is a multiple of 32 and of kPolyLanes: a site's lanes share a
@@ -970,18 +1005,33 @@ __global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int step = 1; step < kPolyLanes; step <<= 1) {
-        shfl_mat<N>(A, P, lane + step < 32 ? lane + step : lane);
+        shfl_mat<N>(A, Pm, lane + step < 32 ? lane + step : lane);
         if ((k & (2 * step - 1)) == 0) {
-            mmul(P, A, T);
-            P = T;
+            mmul(Pm, A, T);
+            Pm = T;
         }
     }
-    double re = 0.0, im = 0.0;
+    re = 0.0;
+    im = 0.0;
     if (valid && k == 0) {
-        const cx<double> tr = mtrace(P);
+        const cx<double> tr = mtrace(Pm);
         re = tr.re;
         im = tr.im;
     }
+}
+
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials, double* out, unsigned* counters,
+                                                   const unsigned* slot)
+{
+    __shared__ DD sh[32];
+    const int b = blockIdx.x;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    double re, im;
+    polyakov_item<N, R, LAYOUT, LD_NC>(L, g, w, re, im);
     block_sum(re, partials + (size_t)b * 4, sh);
     block_sum(im, partials + (size_t)b * 4 + 2, sh);
     if (out) finalize_if_last(bv, l, partials, 2, out, counters, slot);
@@ -1172,6 +1222,247 @@ __global__ void __launch_bounds__(256) k_unpack(BatchView bv, double2* canon)
 }
 
 // ---------------------------------------------------------------------------
+// Resident sweeps: one cooperative launch advances a lattice through many
+// sweeps and measures it after each, with grid barriers where the launched
+// path has launch boundaries (a small lattice's phase is a few microseconds,
+// so the boundaries are a large share of it).  Each stage walks the
+// decomposition of the kernel it stands for (virtual CTA vb of that launch
+// runs on CTA vb mod grid), and every stage reads the links through L2 only
+// (their lines in an SM's L1 may be stale after a barrier), so the links,
+// the counters and the measurements have the bits of the launched path.
+SUN_DEV unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+SUN_DEV unsigned ld_relaxed(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+SUN_DEV void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// spins of one barrier wait at most (a second bound beside wait_ns)
+constexpr unsigned kBarrierMaxSpins = 1u << 24;
+
+// Split grid barriers on one arrival count: barrier k is complete once
+// *a.bar >= G (k + 1), G the grid size (the count only grows during a
+// launch, so nothing is reset between barriers).  A CTA arrives when its
+// part of the stage is done (its threads' writes, then one release fence and
+// an atomic add by thread 0) and waits only where it needs the stage
+// complete -- an update just before the staple of the direction the
+// previous phase wrote, as a programmatic dependent launch does.  A wait
+// polls with relaxed loads and ends with an acquire fence; it is bounded by
+// a.wait_ns and kBarrierMaxSpins: one that runs out sets *a.status, every
+// later wait then returns at once, and each CTA leaves at its next
+// arrival.  Returns the count seen (0 when the wait failed).
+SUN_DEV unsigned wait_count(const unsigned* count, unsigned target, int* status, unsigned long long wait_ns)
+{
+    unsigned c = ld_relaxed(count);
+    if (c < target) {
+        const unsigned long long t0 = global_ns();
+        for (unsigned it = 0;; ++it) {
+            c = ld_relaxed(count);
+            if (c >= target) break;
+            if (ld_relaxed(reinterpret_cast<const unsigned*>(status)) != 0u) return 0u;
+            if (it >= kBarrierMaxSpins || global_ns() - t0 > wait_ns) {
+                atomicExch(status, 1);
+                return 0u;
+            }
+            if (it >= 64) __nanosleep(32);
+        }
+    }
+    fence_acq_rel();
+    return c;
+}
+// The waits of one update phase of a resident launch: `pre` the arrival
+// count at which the phase two back is complete (before any staple), `dep`
+// the count at which the previous phase is complete (before the staple of
+// its direction); 0: nothing to wait for.  Called by all lanes of a warp at
+// once: lane 0 polls (unless the CTA has seen the count already, *seen),
+// records the count seen, and the warp proceeds together.
+struct ResidentDep {
+    const unsigned* count;
+    int* status;
+    unsigned long long wait_ns;
+    unsigned pre, dep_target;
+    unsigned* seen;
+    SUN_DEV void wait_for(unsigned target) const
+    {
+        if ((threadIdx.x & 31) == 0 && *reinterpret_cast<volatile unsigned*>(seen) < target) {
+            const unsigned c = wait_count(count, target, status, wait_ns);
+            if (c) atomicMax(seen, c);
+        }
+        __syncwarp();
+    }
+    SUN_DEV int dep(int mu) const { return dep_target ? ((mu + 3) & 3) : -1; }
+    SUN_DEV void start(int) const
+    {
+        if (pre) wait_for(pre);
+    }
+    SUN_DEV void wait() const { wait_for(dep_target); }
+};
+// this CTA arrives at the barrier of the stage it has finished (its
+// threads' writes, then a release fence and the count), once the arrival
+// count has reached `need` (the stage before complete: seen by one of its
+// warps already, or waited for here), so the arrivals of one barrier never
+// run ahead of the barrier before.  The test hook: the CTA a.skip_arrive
+// leaves at its first arrival without arriving.  False: leave.
+SUN_DEV bool cta_arrive(const ResidentArgs& a, unsigned need, unsigned* seen, bool& first)
+{
+    __shared__ int go;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = !((int)blockIdx.x == a.skip_arrive && first);
+        if (ok && *seen < need) {
+            const unsigned c = wait_count(a.bar, need, a.status, a.wait_ns);
+            if (c) *seen = c;
+            ok = c != 0u;
+        }
+        if (ok) {
+            fence_acq_rel();
+            atomicAdd(a.bar, 1u);
+        }
+        go = ok;
+    }
+    first = false;
+    __syncthreads();
+    return go != 0;
+}
+// the whole CTA waits until the arrival count reaches target.  False: leave.
+SUN_DEV bool cta_wait(const ResidentArgs& a, unsigned target, unsigned* seen)
+{
+    __shared__ int go;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned c = *seen >= target ? *seen : wait_count(a.bar, target, a.status, a.wait_ns);
+        if (c) *seen = c;
+        go = c != 0u;
+    }
+    __syncthreads();
+    return go != 0;
+}
+
+// one update phase over the update decomposition, on the CTAs of one set
+// (CTA rank r of P in the set walks virtual CTAs r, r + P, ...): ROWS the
+// row-split body of k_update_rows (CTAs of 4 warps, 32 / N half-sites per
+// warp), else one thread per half-site as k_update
+template <int N, class R, int LAYOUT, int MODE, bool ROWS>
+SUN_DEV void resident_phase(const ResidentArgs& a, const Geom& g, const LatDev& L, int parity, int mu,
+                            unsigned hb_offset, const ResidentDep& dp, int rank, int P)
+{
+    const InjView none{nullptr, 0, nullptr};
+    cx<R>* base = reinterpret_cast<cx<R>*>(L.links);
+    const uint32_t stride = 4u * (uint32_t)g.V;
+    for (int vb = rank; vb < a.upd.nblocks; vb += P) {
+        if constexpr (ROWS) {
+            constexpr int SPW = 32 / N;
+            const int first = vb * ((int)(blockDim.x >> 5) * SPW) + (int)(threadIdx.x >> 5) * SPW;
+            if (first < g.halfV) update_rows_warp<N, R, LAYOUT, MODE>(g, L, first, parity, mu, hb_offset, none, dp);
+        } else {
+            // every lane of a warp with work runs the update (the waits are
+            // warp-wide); a lane past the end computes a copy of the last
+            // half-site and stores nothing
+            const int id0 = vb * (int)blockDim.x + (int)threadIdx.x;
+            if (id0 - (int)(threadIdx.x & 31) < g.halfV) {
+                const bool valid = id0 < g.halfV;
+                update_site<N, R, LAYOUT, MODE>(
+                    g, L, valid ? id0 : g.halfV - 1, parity, mu, hb_offset, none, dp,
+                    [&](uint32_t i, int e) { return ld_elem<R, LD_CG>(base + i + e * stride); },
+                    [&](uint32_t i, int e, cx<R> v) {
+                        if (valid) st_elem<R>(base + i + e * stride, v);
+                    });
+            }
+        }
+    }
+}
+
+// The grid is two sets of P CTAs that take the update phases in turn, as
+// launched phases overlap under programmatic dependent launch: set j mod 2
+// runs phase j, summing the staples that do not read the previous phase's
+// direction while phase j - 1 still runs on the other set, and waiting for
+// it only before the last staple.  Barrier arithmetic: every CTA tracks
+// `done`, the arrival count at which the latest barrier completes, and
+// `prev` the one before; a phase adds P arrivals, a stage run by the whole
+// grid (reunitarization, measurements) adds 2 P.
+template <int N, class R, int LAYOUT, bool ROWS>
+__global__ void __launch_bounds__(128) k_sweeps_resident(ResidentArgs a)
+{
+    __shared__ DD sh[32];
+    __shared__ unsigned seen;  // the largest arrival count this CTA has seen reached
+    if (threadIdx.x == 0) seen = 0u;
+    __syncthreads();
+    const LatDev& L = a.upd.lats[0];
+    const Geom g = geom_of(L);
+    const unsigned P = gridDim.x / 2u;
+    const int set = blockIdx.x >= P, rank = (int)blockIdx.x - set * (int)P;
+    unsigned done = 0u, prev = 0u;
+    bool first = true;
+    // the counters stay as they were during the launch (the heatbath pass of
+    // sweep i is the lattice's pass count plus i n_hb + h, as the launched
+    // path counts it); CTA 0 advances them at the end
+    const unsigned sweeps0 = __ldcg(L.state + 1);
+    for (int sw = 0; sw < a.n_sweeps; ++sw) {
+        int j = 0;  // phase of the sweep (8 per pass: an even count, so each sweep starts on set 0)
+        for (int pass = 0; pass < a.n_hb + a.n_or; ++pass) {
+            const bool hb = pass < a.n_hb;
+            const unsigned off = hb ? (unsigned)(sw * a.n_hb + pass) : 0u;
+            for (int par = 0; par < 2; ++par)
+                for (int mu = 0; mu < 4; ++mu, ++j) {
+                    if ((j & 1) == set) {
+                        const ResidentDep dp{a.bar, a.status, a.wait_ns, prev, done, &seen};
+                        if (hb) resident_phase<N, R, LAYOUT, MODE_HB, ROWS>(a, g, L, par, mu, off, dp, rank, (int)P);
+                        else resident_phase<N, R, LAYOUT, MODE_OR, ROWS>(a, g, L, par, mu, 0u, dp, rank, (int)P);
+                        if (!cta_arrive(a, done, &seen, first)) return;
+                    }
+                    prev = done;
+                    done += P;
+                }
+        }
+        // reunitarization on the lattice's schedule, as k_reunit(only_due)
+        const unsigned swn = sweeps0 + (unsigned)sw + 1u;
+        if (L.reunit_every > 0 && swn % (unsigned)L.reunit_every == 0u) {
+            if (!cta_wait(a, done, &seen)) return;
+            for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < 4 * g.V; w += gridDim.x * blockDim.x)
+                reunit_link<N, R, LAYOUT, LD_CG>(L, w);
+            if (!cta_arrive(a, done, &seen, first)) return;
+            prev = done;
+            done += gridDim.x;
+        }
+        // plaquette and Polyakov loop, partials of k_plaquette's and
+        // k_polyakov's CTAs, finalized as their last CTA does
+        if (!cta_wait(a, done, &seen)) return;
+        double* ppart = a.partials + (size_t)a.plaq.nblocks * 4;
+        for (int vb = blockIdx.x; vb < a.plaq.nblocks; vb += gridDim.x) {
+            double sp, tp;
+            plaquette_item<N, R, LAYOUT, LD_CG>(L, g, vb * (int)blockDim.x + (int)threadIdx.x, sp, tp);
+            block_sum(sp, a.partials + (size_t)vb * 4, sh);
+            block_sum(tp, a.partials + (size_t)vb * 4 + 2, sh);
+        }
+        for (int vb = blockIdx.x; vb < a.poly.nblocks; vb += gridDim.x) {
+            double re, im;
+            polyakov_item<N, R, LAYOUT, LD_CG>(L, g, vb * (int)blockDim.x + (int)threadIdx.x, re, im);
+            block_sum(re, ppart + (size_t)vb * 4, sh);
+            block_sum(im, ppart + (size_t)vb * 4 + 2, sh);
+        }
+        if (!cta_arrive(a, done, &seen, first)) return;
+        prev = done;
+        done += gridDim.x;
+        if (!cta_wait(a, done, &seen)) return;
+        // the partials are written again only after the next sweep's
+        // barriers, which these CTAs reach after their finalize
+        if (blockIdx.x == 0 && threadIdx.x < 32) finalize_partials(a.partials, 0, a.plaq.nblocks, 2, a.out_plaq + 2 * sw);
+        if (blockIdx.x == gridDim.x - 1 && threadIdx.x < 32) finalize_partials(ppart, 0, a.poly.nblocks, 2, a.out_poly + 2 * sw);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        L.state[0] += (unsigned)(a.n_sweeps * a.n_hb);
+        L.state[1] += (unsigned)a.n_sweeps;
+        L.state[2] = 1u;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host launch wrappers: runtime (precision, layout) -> template instance.
 // SOA12 and SOA8 exist for N == 3 only (the reference silently falls back to
 // SOA for other N, gaugearray.h:127-137; the C ABI rejects them instead).
@@ -1274,6 +1565,45 @@ cudaError_t Ops<N>::update_tile(int fp64, int layout, int mode, const BatchView&
             else e = launch_tile<N, float, MODE_HB_INJECTED>(bv, parity, mu, hb_offset, inj, pdl, s);
         }
         return e != cudaSuccess ? e : cudaGetLastError();
+    }
+}
+
+template <int N>
+cudaError_t Ops<N>::sweeps_resident(int fp64, int layout, int rows, const ResidentArgs& a, int grid, cudaStream_t s)
+{
+    if constexpr (N > 4) {
+        return cudaErrorInvalidValue;  // N = 6 runs the tiled update, which has no resident form
+    } else {
+        cudaError_t e = cudaSuccess;
+        ResidentArgs args = a;
+        void* params[] = {&args};
+#define CALL(R_, L_)                                                                                             \
+    e = rows ? cudaLaunchCooperativeKernel((const void*)k_sweeps_resident<N, R_, L_, true>, dim3(grid), dim3(128), \
+                                           params, 0, s)                                                          \
+             : cudaLaunchCooperativeKernel((const void*)k_sweeps_resident<N, R_, L_, false>, dim3(grid),          \
+                                           dim3(128), params, 0, s)
+        SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
+}
+
+template <int N> int Ops<N>::resident_capacity(int fp64, int layout, int rows)
+{
+    if constexpr (N > 4) {
+        return 0;
+    } else {
+        int dev = 0, sms = 0, per = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return 0;
+        cudaError_t e = cudaSuccess;
+#define CALL(R_, L_)                                                                                            \
+    e = rows ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweeps_resident<N, R_, L_, true>, 128, 0) \
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweeps_resident<N, R_, L_, false>, 128, 0)
+        SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+        return e == cudaSuccess ? per * sms : 0;
     }
 }
 

@@ -64,6 +64,24 @@ constexpr int kPolyLanes = 8;
 constexpr int kPlaneSplitMaxV = 1 << 17;
 __host__ __device__ inline int plaquette_items(int V) { return V < kPlaneSplitMaxV ? ((V + 31) / 32) * 192 : V; }
 
+// Many sweeps of one lattice in one cooperative launch (k_sweeps_resident):
+// the update phases, the reunitarization and the measurements separated by
+// grid barriers instead of launch boundaries.  Every CTA of the launch is
+// resident; the kernel walks the launched kernels' CTA decompositions
+// (virtual CTAs) so each result has the bits of the launched path.
+struct ResidentArgs {
+    BatchView upd;            // the update's decomposition (one lattice)
+    BatchView plaq, poly;     // k_plaquette's and k_polyakov's (CTAs of 128 threads)
+    int n_hb, n_or, n_sweeps;
+    double* partials;         // plaquette partials (4 doubles per virtual CTA), then Polyakov ones
+    double* out_plaq;         // per sweep: spatial and temporal sums
+    double* out_poly;         // per sweep: real and imaginary trace sums
+    unsigned* bar;            // arrivals at the grid barriers; zero at launch
+    int* status;              // set to 1 when a barrier wait runs out
+    unsigned long long wait_ns;  // limit of one barrier wait
+    int skip_arrive;          // test hook: CTA that leaves at its first barrier without arriving (-1: none)
+};
+
 template <int N> struct Ops {
     // one checkerboard phase (parity, mu) of heatbath or overrelaxation;
     // hb_offset is added to the lattice's pass counter (heatbath pass index
@@ -85,6 +103,13 @@ template <int N> struct Ops {
     // the same bits as update()
     static cudaError_t update_tile(int fp64, int layout, int mode, const BatchView& bv, int parity, int mu,
                                    unsigned hb_offset, const InjView& inj, int pdl, cudaStream_t s);
+    // n sweeps of one lattice and their measurements in one cooperative
+    // launch of `grid` CTAs of 128 threads (k_sweeps_resident); rows: the
+    // row-split update body (k_update_rows) instead of one thread per
+    // half-site.  capacity: the most CTAs that can be resident at once.
+    static cudaError_t sweeps_resident(int fp64, int layout, int rows, const ResidentArgs& a, int grid,
+                                       cudaStream_t s);
+    static int resident_capacity(int fp64, int layout, int rows);
     static cudaError_t cold(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
     static cudaError_t hot(int fp64, int layout, const BatchView& bv, int block, cudaStream_t s);
     // FP64 reunitarization; only_due: skip lattices whose sweep counter is not

@@ -35,3 +35,37 @@ def test_sweep_measure_matches_sweep_by_sweep_calls(ctx, case):
     po, lo = O.plaquette(U, X), O.polyakov(U, X)
     assert abs(pa[-1, 0] - po[0]) < 1e-12 and abs(pa[-1, 1] - po[1]) < 1e-12
     assert abs(la[-1] - (lo[0] + 1j * lo[1])) < 1e-12
+
+
+def test_captured_measurements_keep_their_partials():
+    """The captured sweep-and-measure graph (resident sweeps off) replayed
+    after Wilson loops up to 4x4, which need more CTA partials than the
+    graph's measurements: the replays still give the sweep-by-sweep values."""
+    import os
+    from sun_b200 import Context, OnePolyakovLoop, PlaquetteCUB, Sweep, SweepMeasure, WilsonLoop, gauge
+    old = os.environ.get("SUN_B200_RESIDENT")
+    os.environ["SUN_B200_RESIDENT"] = "0"
+    try:
+        c = Context(0)
+    finally:
+        if old is None:
+            del os.environ["SUN_B200_RESIDENT"]
+        else:
+            os.environ["SUN_B200_RESIDENT"] = old
+    try:
+        a, b = (gauge(c, N=3, dims=(8, 8, 8, 8), beta=6.0, atype=0, evenodd=True, prec="f64", seed=17)
+                for _ in range(2))
+        a.Init(hot=True)
+        b.Init(hot=True)
+        SweepMeasure(a, 1, 4, 2)
+        Sweep(b, 1, 4, 2)
+        wa, wb = WilsonLoop(a, 4, 4), WilsonLoop(b, 4, 4)
+        assert np.array_equal(wa, wb)
+        pa, la = SweepMeasure(a, 1, 4, 3)
+        for i in range(3):
+            Sweep(b, 1, 4, 1)
+            p, l = PlaquetteCUB(b).Run(), OnePolyakovLoop(b).Run()
+            assert pa[i, 0] == p.real and pa[i, 1] == p.imag and la[i] == l, i
+        assert np.array_equal(a.get_image(), b.get_image())
+    finally:
+        c.close()
