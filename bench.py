@@ -668,13 +668,16 @@ def serving_bench(ctx, rate=50.0, window=3.0, max_active=256):
         if not done and srv.pending() == (0, 0) and nxt < len(pending):
             time.sleep(max(0.0, min(0.01, pending[nxt]["t"] - (time.perf_counter() - t0))))
     wall = time.perf_counter() - t0
+    steps = srv.stats()
     srv.close()
     ok = [r for r in results if r["status"] == 0]
     lat = np.array([r["finish_s"] - r["submit_s"] for r in ok])
     upd = sum(r["link_updates"] for r in ok)
     out = {"jobs": len(jobs), "completed": len(ok), "arrival_rate_per_s": rate, "window_s": window,
            "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
-           "link_updates_per_s": upd / wall, "wall_s": wall, "max_active": max_active}
+           "link_updates_per_s": upd / wall, "wall_s": wall, "max_active": max_active,
+           "steps": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in steps.items()},
+           "gpu_busy_frac": steps["sweep_gpu_s"] / wall}
     if len(ok) == len(jobs):
         # compulsory bytes: 9 link-records per update (48 B SU(3) 12-parameter,
         # 8 N^2 B full FP32 links)

@@ -306,6 +306,17 @@ sun_status sun_server_submit(sun_server *s, const sun_job *job, int64_t *id);
  * written to out[0..cap) */
 sun_status sun_server_step(sun_server *s, sun_result *out, int cap, int *n_done);
 sun_status sun_server_pending(const sun_server *s, int *queued, int *active);
+/* where the server's steps spent their time (seconds, summed over steps):
+ * GPU time of the sweeps (CUDA events), and host time queueing the sweeps
+ * (batch graph captures included), admitting jobs (lattice setup),
+ * waiting for the sweeps, measuring and retiring finished jobs, and adding
+ * admitted jobs to their batches */
+typedef struct {
+    int64_t steps, sweeps;    /* steps with sweeps; K summed over them */
+    double sweep_gpu_s;
+    double enqueue_s, admit_s, wait_s, retire_s, join_s;
+} sun_server_stats;
+sun_status sun_server_get_stats(const sun_server *s, sun_server_stats *out);
 /* bytes a job needs on the device (links + measurement scratch) */
 sun_status sun_job_footprint(const sun_job *job, size_t *bytes);
 /* override the admission budget (default: the context's, sun_ctx_hbm_budget) */

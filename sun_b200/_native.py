@@ -40,6 +40,11 @@ class SunJob(C.Structure):
                 ("precision", C.c_int), ("layout", C.c_int), ("reunit_every", C.c_int)]
 
 
+class SunServerStats(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("sweeps", C.c_int64), ("sweep_gpu_s", C.c_double), ("enqueue_s", C.c_double),
+                ("admit_s", C.c_double), ("wait_s", C.c_double), ("retire_s", C.c_double), ("join_s", C.c_double)]
+
+
 class SunResult(C.Structure):
     _fields_ = [("id", C.c_int64), ("status", C.c_int), ("plaquette", C.c_double * 2),
                 ("polyakov", C.c_double * 2), ("wilson", C.c_double * (2 * 9 * 9)),
@@ -105,6 +110,7 @@ _SIGS = {
     "sun_server_submit": [_vp, C.POINTER(SunJob), C.POINTER(C.c_int64)],
     "sun_server_step": [_vp, C.POINTER(SunResult), C.c_int, C.POINTER(C.c_int)],
     "sun_server_pending": [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "sun_server_get_stats": [_vp, C.POINTER(SunServerStats)],
     "sun_job_footprint": [C.POINTER(SunJob), C.POINTER(C.c_size_t)],
     "sun_server_set_budget": [_vp, C.c_size_t],
     "sun_admit_count": [C.POINTER(C.c_size_t), C.c_int, C.c_size_t, C.c_size_t, C.c_int, C.POINTER(C.c_int)],

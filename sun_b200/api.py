@@ -431,6 +431,13 @@ class Server:
         check(lib().sun_server_pending(self.h, C.byref(q), C.byref(a)))
         return q.value, a.value
 
+    def stats(self) -> dict:
+        """Where the steps spent their time (sun_server_get_stats)."""
+        from ._native import SunServerStats
+        st = SunServerStats()
+        check(lib().sun_server_get_stats(self.h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in SunServerStats._fields_}
+
     def close(self) -> None:
         if self.h:
             lib().sun_server_destroy(self.h)

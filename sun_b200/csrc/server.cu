@@ -108,6 +108,7 @@ struct sun_server {
     cudaStream_t work = nullptr, side = nullptr;
     cudaEvent_t t_sweep[2] = {nullptr, nullptr};
     std::vector<Active> admitted;  // set up during the last step, not yet in a batch
+    sun_server_stats stats{};
 
     ~sun_server()
     {
@@ -222,10 +223,23 @@ sun_status sun_server_pending(const sun_server* s, int* queued, int* active)
     return SUN_OK;
 }
 
+sun_status sun_server_get_stats(const sun_server* s, sun_server_stats* out)
+{
+    if (!s || !out) return SUN_ERR_INVALID_ARG;
+    *out = s->stats;
+    return SUN_OK;
+}
+
 sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
 {
     if (!s || !n_done || (cap > 0 && !out)) return SUN_ERR_INVALID_ARG;
     auto emit = [&](const sun_result& r) { s->outbox.push_back(r); };
+    double tick = s->now();
+    auto lap = [&](double& acc) {
+        const double t = s->now();
+        acc += t - tick;
+        tick = t;
+    };
     // 1. queue up to K sweeps of every active job, batched per (n_hb, n_or),
     // on the work stream without waiting; a job with fewer sweeps left
     // stops at its own count (device-side limit)
@@ -244,6 +258,7 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
             if (st != SUN_OK) return st;
         }
     }
+    lap(s->stats.enqueue_s);
     // 2. meanwhile admit queued jobs: their lattices are allocated and
     // initialized on the side stream while the GPU sweeps, and join their
     // batches after this step's sweeps
@@ -294,12 +309,17 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
             s->admitted.push_back(a);
         }
     }
+    lap(s->stats.admit_s);
     // 3. the sweeps done: seconds per sweep (CUDA events) for the next K
     if (k > 0) {
         cudaEventRecord(s->t_sweep[1], s->work);
         if (cudaEventSynchronize(s->t_sweep[1]) != cudaSuccess) return SUN_ERR_CUDA;
+        lap(s->stats.wait_s);
         float ms = 0;
         cudaEventElapsedTime(&ms, s->t_sweep[0], s->t_sweep[1]);
+        s->stats.steps += 1;
+        s->stats.sweeps += k;
+        s->stats.sweep_gpu_s += 1e-3 * ms;
         const double per = 1e-3 * ms / k;
         s->sweep_s = s->sweep_s > 0 ? 0.5 * (s->sweep_s + per) : per;
         for (auto& a : s->active) a.remaining = std::max(0, a.remaining - k);
@@ -359,6 +379,7 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
         }
     }
     s->active.swap(keep);
+    lap(s->stats.retire_s);
     // 5. the jobs admitted during this step join their batches (from the
     // next step on); jobs without sweeps are finished as they stand
     for (auto& a : s->admitted) {
@@ -372,6 +393,7 @@ sun_status sun_server_step(sun_server* s, sun_result* out, int cap, int* n_done)
         s->active.push_back(a);
     }
     s->admitted.clear();
+    lap(s->stats.join_s);
     int done = 0;
     while (done < cap && !s->outbox.empty()) {
         out[done++] = s->outbox.front();

@@ -527,6 +527,28 @@ def test_server_budget_defaults_to_the_context_budget():
         s.close()
 
 
+def test_server_step_statistics(ctx):
+    """sun_server_get_stats: the steps' sweeps, their GPU time and the host
+    time per part add up (the parts are disjoint pieces of the steps' wall
+    time)."""
+    import time
+    from sun_b200 import Server, make_job
+    s = Server(ctx, max_active=8)
+    for i in range(3):
+        s.submit(make_job(N=3, dims=(8, 8, 8, 8), beta=5.8, sweeps=6 + i, seed=40 + i))
+    t0, res = time.perf_counter(), []
+    while len(res) < 3:
+        res += s.step()
+    wall = time.perf_counter() - t0
+    st = s.stats()
+    s.close()
+    assert all(r["status"] == 0 for r in res)
+    assert st["steps"] >= 1 and 8 <= st["sweeps"] <= 8 * st["steps"] + 8
+    assert st["sweep_gpu_s"] > 0.0
+    parts = st["enqueue_s"] + st["admit_s"] + st["wait_s"] + st["retire_s"] + st["join_s"]
+    assert 0.0 < parts <= wall + 1e-3
+
+
 def test_batch_of_uneven_shapes_with_graph(ctx):
     from sun_b200 import Batch, Sweep
     batch, alone, mixed = Batch(ctx), [], []
