@@ -450,13 +450,23 @@ def main():
     e1.record(stream)
     stream.synchronize()
     t_hb = e0.elapsed_time(e1) / 1e3 / (8 * n_hbp)
+    # the spread of single sweeps: p50 / p99 over repeats, each sweep
+    # bracketed by its own events
+    n_rep = 20
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(n_rep + 1)]
+    evs[0].record(stream)
+    for i in range(n_rep):
+        sweeps(g, 1)
+        evs[i + 1].record(stream)
+    stream.synchronize()
+    per_sweep = sorted(evs[i].elapsed_time(evs[i + 1]) for i in range(n_rep))
     clk = clocks.stop()
     accuracy = None
     if rank == 0 and not args.no_cpu:
         # the accuracy report on the configuration after 500 sweeps (the
         # length of the FP32-against-FP64 run of the 32^4 configuration),
         # besides the 10 overrelaxation and 4 heatbath passes timed above
-        done = args.warmup + args.steps
+        done = args.warmup + args.steps + n_rep
         if done < 500:
             sweeps(g, 500 - done)
         accuracy = accuracy_report(ctx, g, stream)
@@ -546,6 +556,8 @@ def main():
                    "l2": "inputs larger than L2 (201 MB link image vs 126 MB L2)", "parallelism": "replicas"},
         "gpu_launches": args.steps * 42,
         "clocks": clk,
+        "sweep_ms": {"p50": per_sweep[n_rep // 2], "p99": per_sweep[-1], "min": per_sweep[0], "repeats": n_rep,
+                     "how": "single sweeps after the timed region, CUDA events around each"},
     }
     peak, peak_kind = measured_hbm()
     bytes_or = (V // 2) * 9 * LINK_RECORD["SOA12_f32"]

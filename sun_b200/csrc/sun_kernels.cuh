@@ -429,12 +429,16 @@ __global__ void __launch_bounds__(128) k_update_rows(BatchView bv, int parity, i
 // per site spills kilobytes.
 //
 // Shared memory (dynamic, tile_smem_bytes): B and D staging, N*N complex x
-// 32 sites each, then the staple sum S; U aliases the B/D staging once the
-// staples are summed.  Element e of a matrix sits at [e][lane]: a warp's
-// access to one element is 32 consecutive complex numbers (no bank
-// conflicts).
+// 32 sites each; once the staples are summed, U takes the place of B and
+// the staple sum S that of D.  Element e of a matrix sits at [e][lane]: a
+// warp's access to one element is 32 consecutive complex numbers (no bank
+// conflicts).  Measured on B200 (SU(6) sweeps): with S in a third array,
+// FP64 24^4 took 17.4 ms against 14.8 ms (FP32 7.86 against 7.75 ms);
+// CTAs of one 32-site tile per warp, each warp then updating its own tile
+// so that none waits for warp 0, took 8.73 ms (FP32) and 19.2 ms (FP64):
+// other CTAs already fill those waits, and the larger CTAs fit fewer per SM.
 constexpr int kTileSites = 32;
-template <int N, class R> constexpr int tile_smem_bytes() { return 3 * N * N * kTileSites * (int)sizeof(cx<R>); }
+template <int N, class R> constexpr int tile_smem_bytes() { return 2 * N * N * kTileSites * (int)sizeof(cx<R>); }
 // CTAs per SM the tiled kernel's registers are capped for (FP32; 0: no cap,
 // the compiler's own choice -- 72 registers for overrelaxation, 96 for the
 // heatbath; FP64 is uncapped).  Caps for 4 to 6 CTAs per SM measured no
@@ -452,9 +456,11 @@ template <class R, int MODE> struct TileOccupancy {
 // Rows of the link matrices per warp (N / rows warps per CTA): each element
 // staged in shared memory is read once for all of a warp's rows, so more
 // rows per warp mean fewer shared-memory reads and fewer, fuller warps.
-// Measured on B200 (SU(6) sweeps, ms, 1 / 2 / 3 rows per warp): FP32 16^4
-// 2.01 / 1.71 / 1.95, 24^4 9.60 / 7.86 / 7.79; FP64 16^4 4.59 / 4.31 / 3.51,
-// 24^4 21.8 / 20.9 / 17.4.  All give the same bits.
+// Measured on B200 (SU(6) sweeps, ms, 1 / 2 / 3 rows per warp, S in a
+// third array): FP32 16^4 2.01 / 1.71 / 1.95, 24^4 9.60 / 7.86 / 7.79; FP64
+// 16^4 4.59 / 4.31 / 3.51, 24^4 21.8 / 20.9 / 17.4.  With S in D's place:
+// FP32 2 / 3 rows 12^4 0.67 / 0.76, 16^4 1.68 / 1.91, 24^4 7.84 / 7.52; FP64
+// 3 / 2 rows 16^4 3.10 / 4.30, 24^4 14.9 / 20.8.  All give the same bits.
 #ifndef SUN_TILE_RPW_F32
 #define SUN_TILE_RPW_F32 2
 #endif
@@ -477,8 +483,8 @@ __global__ void __launch_bounds__(32 * N / tile_rpw<N, R>(), (TileOccupancy<R, M
     extern __shared__ __align__(16) unsigned char tile_raw[];
     C(*const Bs)[kTileSites] = reinterpret_cast<C(*)[kTileSites]>(tile_raw);
     C(*const Ds)[kTileSites] = Bs + N * N;
-    C(*const Ss)[kTileSites] = Ds + N * N;
-    C(*const Us)[kTileSites] = Bs;  // after the staple sum
+    C(*const Ss)[kTileSites] = Ds;  // after the staple sum
+    C(*const Us)[kTileSites] = Bs;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const int b = blockIdx.x;
