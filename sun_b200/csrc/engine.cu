@@ -191,7 +191,7 @@ struct sun_lattice {
     // meas_part: the captured measurements' CTA partials, owned by the graph
     // (a shared scratch buffer could be reallocated under it by a later
     // call that needs more partials)
-    DevBuf meas, slot, meas_part;
+    DevBuf meas, slot, meas_part, meas_cnt;
     ~sun_lattice();
 };
 
@@ -1122,7 +1122,12 @@ static bool solo_measure_graph(sun_lattice* l, Group& g, int n_hb, int n_or, siz
     if (n_or > 0) upd_view(g, update_block(c, g, MODE_OR, s), s);
     if (re) g.view(WORK_LINKS, c->blk_links, s);
     BatchView vp = g.view(WORK_PLANES, c->blk_sites, s), vl = g.view(WORK_POLY8, c->blk_sites, s);
-    l->meas_part.ensure(sizeof(double) * 4 * (size_t)std::max(1, std::max(vp.nblocks, vl.nblocks)));
+    // CTAs of 128 threads: the plaquette and the Polyakov loop in one launch
+    // (own partials and counters: the two parts run side by side)
+    const bool fused = c->blk_sites == 128;
+    l->meas_part.ensure(sizeof(double) * 4 * (size_t)std::max(1, vp.nblocks + vl.nblocks));
+    l->meas_cnt.ensure(sizeof(unsigned) * 3);
+    ck(cudaMemsetAsync(l->meas_cnt.p, 0, sizeof(unsigned) * 3, s), "counters");
     if (g.counters_n < g.lats.size()) {
         g.counters.ensure(sizeof(unsigned) * g.lats.size());
         ck(cudaMemsetAsync(g.counters.p, 0, sizeof(unsigned) * g.lats.size(), s), "counters");
@@ -1140,9 +1145,15 @@ static bool solo_measure_graph(sun_lattice* l, Group& g, int n_hb, int n_or, siz
     ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "capture");
     try {
         group_sweep(c, g, n_hb, n_or, true, re, cs);
-        OPS_CALL(g.N, plaquette, g.fp64, g.layout, vp, c->blk_sites, part, out_p, cnt, slot, cs);
-        OPS_CALL(g.N, polyakov, g.fp64, g.layout, vl, c->blk_sites, part, out_l, cnt, slot, cs);
-        ck(launch_bump(slot, cs), "bump");
+        if (fused) {
+            unsigned* mc = reinterpret_cast<unsigned*>(l->meas_cnt.p);
+            OPS_CALL(g.N, plaq_poly, g.fp64, g.layout, vp, vl, part, part + 4 * (size_t)vp.nblocks, out_p, out_l, mc,
+                     mc + 1, slot, mc + 2, cs);
+        } else {
+            OPS_CALL(g.N, plaquette, g.fp64, g.layout, vp, c->blk_sites, part, out_p, cnt, slot, cs);
+            OPS_CALL(g.N, polyakov, g.fp64, g.layout, vl, c->blk_sites, part, out_l, cnt, slot, cs);
+            ck(launch_bump(slot, cs), "bump");
+        }
     } catch (...) {
         cudaStreamEndCapture(cs, &graph);
         cudaStreamDestroy(cs);

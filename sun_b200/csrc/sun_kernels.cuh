@@ -831,7 +831,8 @@ SUN_DEV void finalize_partials(const double* partials, int b0, int b1, int nvals
         if (lane == 0) dst[v] = d.s + d.c;
     }
 }
-SUN_DEV void finalize_if_last(const BatchView& bv, int l, const double* partials, int nvals, double* out,
+// Returns (in every thread) whether this CTA was the one that finalized.
+SUN_DEV bool finalize_if_last(const BatchView& bv, int l, const double* partials, int nvals, double* out,
                               unsigned* counters, const unsigned* slot)
 {
     __shared__ int last;
@@ -842,11 +843,13 @@ SUN_DEV void finalize_if_last(const BatchView& bv, int l, const double* partials
         last = atomicAdd(counters + l, 1u) == n - 1u;
     }
     __syncthreads();
-    if (!last || threadIdx.x >= 32) return;
+    const bool mine = last != 0;
+    if (!mine || threadIdx.x >= 32) return mine;
     __threadfence();
     const size_t row = slot ? (size_t)__ldcg(slot) * (size_t)bv.nlat * nvals : 0;
     finalize_partials(partials, __ldg(bv.begin + l), __ldg(bv.begin + l + 1), nvals, out + row + (size_t)l * nvals);
     if (threadIdx.x == 0) counters[l] = 0u;
+    return mine;
 }
 
 SUN_DEV void block_max(double v, double* out, double* sh)
@@ -1041,6 +1044,41 @@ __global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials
     block_sum(re, partials + (size_t)b * 4, sh);
     block_sum(im, partials + (size_t)b * 4 + 2, sh);
     if (out) finalize_if_last(bv, l, partials, 2, out, counters, slot);
+}
+
+// The plaquette and the Polyakov loop in one launch (the measurements of a
+// replayed sweep-and-measure graph): CTAs below vp.nblocks are k_plaquette's,
+// the others k_polyakov's, with the same partials and finalize, so the same
+// bits; the two run side by side.  Each part's last CTA per lattice writes
+// row *slot; the last of all the finalizing CTAs (joint counts them) then
+// advances *slot for the next replay.
+template <int N, class R, int LAYOUT>
+__global__ void __launch_bounds__(128) k_plaq_poly(BatchView vp, BatchView vl, double* part_p, double* part_l,
+                                                    double* out_p, double* out_l, unsigned* cnt_p, unsigned* cnt_l,
+                                                    unsigned* slot, unsigned* joint)
+{
+    __shared__ DD sh[32];
+    const bool plaq = (int)blockIdx.x < vp.nblocks;
+    const BatchView& bv = plaq ? vp : vl;
+    const int b = plaq ? (int)blockIdx.x : (int)blockIdx.x - vp.nblocks;
+    const int l = find_lat(bv, b);
+    const LatDev& L = bv.lats[l];
+    const Geom g = geom_of(L);
+    const int w = (b - __ldg(bv.begin + l)) * blockDim.x + threadIdx.x;
+    double v0, v1;
+    if (plaq) plaquette_item<N, R, LAYOUT, LD_NC>(L, g, w, v0, v1);
+    else polyakov_item<N, R, LAYOUT, LD_NC>(L, g, w, v0, v1);
+    double* part = plaq ? part_p : part_l;
+    block_sum(v0, part + (size_t)b * 4, sh);
+    block_sum(v1, part + (size_t)b * 4 + 2, sh);
+    const bool fin = finalize_if_last(bv, l, part, 2, plaq ? out_p : out_l, plaq ? cnt_p : cnt_l, slot);
+    if (fin && threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(joint, 1u) == 2u * (unsigned)vp.nlat - 1u) {
+            *joint = 0u;
+            *slot += 1u;
+        }
+    }
 }
 
 // Planar Wilson loops W(r,t), r <= R, t <= T, averaged over the 3 spatial
@@ -1653,6 +1691,19 @@ cudaError_t Ops<N>::polyakov(int fp64, int layout, const BatchView& bv, int bloc
                              double* out, unsigned* counters, const unsigned* slot, cudaStream_t s)
 {
 #define CALL(R_, L_) k_polyakov<N, R_, L_><<<bv.nblocks, block, 0, s>>>(bv, partials, out, counters, slot)
+    SUN_DISPATCH(fp64, layout, CALL);
+#undef CALL
+    return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t Ops<N>::plaq_poly(int fp64, int layout, const BatchView& vp, const BatchView& vl, double* part_p,
+                              double* part_l, double* out_p, double* out_l, unsigned* cnt_p, unsigned* cnt_l,
+                              unsigned* slot, unsigned* joint, cudaStream_t s)
+{
+#define CALL(R_, L_)                                                                                          \
+    k_plaq_poly<N, R_, L_><<<vp.nblocks + vl.nblocks, 128, 0, s>>>(vp, vl, part_p, part_l, out_p, out_l, cnt_p, \
+                                                                    cnt_l, slot, joint)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
     return cudaGetLastError();

@@ -126,6 +126,11 @@ template <int N> struct Ops {
                                  double* out, unsigned* counters, const unsigned* slot, cudaStream_t s);
     static cudaError_t polyakov(int fp64, int layout, const BatchView& bv, int block, double* partials,
                                 double* out, unsigned* counters, const unsigned* slot, cudaStream_t s);
+    // both in one launch (k_plaq_poly; CTAs of 128 threads, vp and vl built
+    // for 128), the last finalize advancing *slot
+    static cudaError_t plaq_poly(int fp64, int layout, const BatchView& vp, const BatchView& vl, double* part_p,
+                                 double* part_l, double* out_p, double* out_l, unsigned* cnt_p, unsigned* cnt_l,
+                                 unsigned* slot, unsigned* joint, cudaStream_t s);
     static cudaError_t wilson(int fp64, int layout, const BatchView& bv, int block, int R, int T,
                               double* partials, cudaStream_t s);
     static cudaError_t unitarity(int fp64, int layout, const BatchView& bv, int block, double* partials,
