@@ -392,7 +392,11 @@ int update_block(sun_ctx* c, Group& g, int mode, cudaStream_t s)
     return best;
 }
 
-void group_sweep(sun_ctx* c, Group& g, int n_hb, int n_or, bool count_sweep, bool reunit, cudaStream_t s)
+// counters_later: the sweep's counter update is left to the launch after
+// it (the fused measurement of a sweep-and-measure graph; only without a
+// reunitarization, which reads the counters)
+void group_sweep(sun_ctx* c, Group& g, int n_hb, int n_or, bool count_sweep, bool reunit, cudaStream_t s,
+                 bool counters_later = false)
 {
     if (g.lats.empty()) return;
     InjView none{nullptr, 0, nullptr};
@@ -417,7 +421,7 @@ void group_sweep(sun_ctx* c, Group& g, int n_hb, int n_or, bool count_sweep, boo
                 for (int mu = 0; mu < 4; ++mu, pdl = c->pdl)
                     launch_update(g, MODE_OR, bor, vor, par, mu, 0u, none, s, pdl);
     }
-    if (n_hb > 0 || count_sweep)
+    if ((n_hb > 0 || count_sweep) && !(counters_later && !reunit))
         ck(launch_end_sweep(reinterpret_cast<const LatDev*>(g.d_lats.p), (int)g.lats.size(), (unsigned)n_hb,
                             count_sweep ? 1u : 0u, s),
            "end_sweep");
@@ -600,16 +604,7 @@ __global__ void k_finalize_max(BatchView bv, const double* partials, double* out
 __global__ void k_end_sweep(const LatDev* lats, int nlat, unsigned n_hb, unsigned inc)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nlat) {
-        unsigned* st = lats[i].state;
-        const unsigned lim = lats[i].sweep_limit;
-        const unsigned adv = lim == 0u || st[1] < lim;
-        if (adv) {
-            st[0] += n_hb;
-            st[1] += inc;
-        }
-        st[2] = adv;
-    }
+    if (i < nlat) advance_counters(lats[i], n_hb, inc);
 }
 
 cudaError_t launch_finalize_sum(const BatchView& bv, const double* partials, int nvals, double* out, cudaStream_t s)
@@ -1144,11 +1139,11 @@ static bool solo_measure_graph(sun_lattice* l, Group& g, int n_hb, int n_or, siz
     cudaGraph_t graph;
     ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "capture");
     try {
-        group_sweep(c, g, n_hb, n_or, true, re, cs);
+        group_sweep(c, g, n_hb, n_or, true, re, cs, fused);
         if (fused) {
             unsigned* mc = reinterpret_cast<unsigned*>(l->meas_cnt.p);
             OPS_CALL(g.N, plaq_poly, g.fp64, g.layout, vp, vl, part, part + 4 * (size_t)vp.nblocks, out_p, out_l, mc,
-                     mc + 1, slot, mc + 2, cs);
+                     mc + 1, slot, mc + 2, re ? -1 : n_hb, cs);
         } else {
             OPS_CALL(g.N, plaquette, g.fp64, g.layout, vp, c->blk_sites, part, out_p, cnt, slot, cs);
             OPS_CALL(g.N, polyakov, g.fp64, g.layout, vl, c->blk_sites, part, out_l, cnt, slot, cs);

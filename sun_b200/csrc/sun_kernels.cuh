@@ -1051,11 +1051,12 @@ __global__ void __launch_bounds__(128) k_polyakov(BatchView bv, double* partials
 // the others k_polyakov's, with the same partials and finalize, so the same
 // bits; the two run side by side.  Each part's last CTA per lattice writes
 // row *slot; the last of all the finalizing CTAs (joint counts them) then
-// advances *slot for the next replay.
+// advances *slot for the next replay and, with end_n_hb >= 0, ends the sweep
+// (the counters, which the measurements do not read).
 template <int N, class R, int LAYOUT>
 __global__ void __launch_bounds__(128) k_plaq_poly(BatchView vp, BatchView vl, double* part_p, double* part_l,
                                                     double* out_p, double* out_l, unsigned* cnt_p, unsigned* cnt_l,
-                                                    unsigned* slot, unsigned* joint)
+                                                    unsigned* slot, unsigned* joint, int end_n_hb)
 {
     __shared__ DD sh[32];
     const bool plaq = (int)blockIdx.x < vp.nblocks;
@@ -1077,6 +1078,8 @@ __global__ void __launch_bounds__(128) k_plaq_poly(BatchView vp, BatchView vl, d
         if (atomicAdd(joint, 1u) == 2u * (unsigned)vp.nlat - 1u) {
             *joint = 0u;
             *slot += 1u;
+            if (end_n_hb >= 0)
+                for (int i = 0; i < vp.nlat; ++i) advance_counters(vp.lats[i], (unsigned)end_n_hb, 1u);
         }
     }
 }
@@ -1699,11 +1702,11 @@ cudaError_t Ops<N>::polyakov(int fp64, int layout, const BatchView& bv, int bloc
 template <int N>
 cudaError_t Ops<N>::plaq_poly(int fp64, int layout, const BatchView& vp, const BatchView& vl, double* part_p,
                               double* part_l, double* out_p, double* out_l, unsigned* cnt_p, unsigned* cnt_l,
-                              unsigned* slot, unsigned* joint, cudaStream_t s)
+                              unsigned* slot, unsigned* joint, int end_n_hb, cudaStream_t s)
 {
 #define CALL(R_, L_)                                                                                          \
     k_plaq_poly<N, R_, L_><<<vp.nblocks + vl.nblocks, 128, 0, s>>>(vp, vl, part_p, part_l, out_p, out_l, cnt_p, \
-                                                                    cnt_l, slot, joint)
+                                                                    cnt_l, slot, joint, end_n_hb)
     SUN_DISPATCH(fp64, layout, CALL);
 #undef CALL
     return cudaGetLastError();

@@ -32,6 +32,20 @@ __host__ __device__ inline bool lat_frozen(const LatDev& L)
 #endif
 }
 
+// The end of a counted sweep: the pass and sweep counters advance by n_hb
+// and inc unless the lattice sits at its sweep limit; state[2] records
+// whether it advanced.
+__device__ inline void advance_counters(const LatDev& L, unsigned n_hb, unsigned inc)
+{
+    unsigned* st = L.state;
+    const unsigned adv = L.sweep_limit == 0u || st[1] < L.sweep_limit;
+    if (adv) {
+        st[0] += n_hb;
+        st[1] += inc;
+    }
+    st[2] = adv;
+}
+
 // A launch over several lattices of one class (same N, precision, layout):
 // CTA b works on lattice l with begin[l] <= b < begin[l+1].
 struct BatchView {
@@ -128,9 +142,11 @@ template <int N> struct Ops {
                                 double* out, unsigned* counters, const unsigned* slot, cudaStream_t s);
     // both in one launch (k_plaq_poly; CTAs of 128 threads, vp and vl built
     // for 128), the last finalize advancing *slot
+    // end_n_hb >= 0: the same launch ends the sweep (advance_counters with
+    // n_hb = end_n_hb, one sweep) after the measurements
     static cudaError_t plaq_poly(int fp64, int layout, const BatchView& vp, const BatchView& vl, double* part_p,
                                  double* part_l, double* out_p, double* out_l, unsigned* cnt_p, unsigned* cnt_l,
-                                 unsigned* slot, unsigned* joint, cudaStream_t s);
+                                 unsigned* slot, unsigned* joint, int end_n_hb, cudaStream_t s);
     static cudaError_t wilson(int fp64, int layout, const BatchView& bv, int block, int R, int T,
                               double* partials, cudaStream_t s);
     static cudaError_t unitarity(int fp64, int layout, const BatchView& bv, int block, double* partials,
