@@ -381,7 +381,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the FP64 and batched side measurements")
     ap.add_argument("--profile-case", default=None,
                     help="run one short workload for a profiler and exit: suN_L (SU(N), L^4, FP32 links, hot "
-                         "start, one sweep of 1 HB + 4 OR), e.g. su6_20")
+                         "start, one sweep of 1 HB + 4 OR), e.g. su6_20, or small8 (SU(3) 8^4 FP64, three sweeps)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -617,12 +617,22 @@ def main():
 
 
 def profile_case(case):
-    """A short workload for a profiler (ncu): SU(N) on L^4, FP32 links (the
-    benchmark's 12-parameter layout for SU(3), full links otherwise), hot
-    start, one sweep of 1 heatbath + 4 overrelaxation passes (8 heatbath
-    then 32 overrelaxation update launches)."""
+    """A short workload for a profiler (ncu): "suN_L" SU(N) on L^4, FP32
+    links (the benchmark's 12-parameter layout for SU(3), full links
+    otherwise), hot start, one sweep of 1 heatbath + 4 overrelaxation passes
+    (8 heatbath then 32 overrelaxation update launches); "small8" the plain
+    small case (SU(3) 8^4 FP64 full links, cold start), three such sweeps."""
     import torch
     from sun_b200 import Context, Sweep, gauge
+    if case == "small8":
+        with Context(0) as ctx:
+            g = gauge(ctx, N=3, dims=(8, 8, 8, 8), beta=6.0, atype=0, evenodd=True, prec="f64", seed=SEED)
+            g.Init(hot=False)
+            Sweep(g, 1, 4, 3)
+            torch.cuda.synchronize()
+            g.Release()
+        print(f"profile case {case}: three sweeps done", flush=True)
+        return
     n, l = case[2:].split("_")
     with Context(0) as ctx:
         g = gauge(ctx, N=int(n), dims=(int(l),) * 4, beta={2: 2.5, 3: 6.0, 4: 11.1, 6: 25.0}[int(n)],
