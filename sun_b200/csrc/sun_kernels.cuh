@@ -1273,10 +1273,11 @@ __global__ void __launch_bounds__(256) k_unpack(BatchView bv, double2* canon)
 // sweeps and measures it after each, with grid barriers where the launched
 // path has launch boundaries (a small lattice's phase is a few microseconds,
 // so the boundaries are a large share of it).  Each stage walks the
-// decomposition of the kernel it stands for (virtual CTA vb of that launch
-// runs on CTA vb mod grid), and every stage reads the links through L2 only
-// (their lines in an SM's L1 may be stale after a barrier), so the links,
-// the counters and the measurements have the bits of the launched path.
+// decomposition of the kernel it stands for (an update phase's virtual CTA
+// v on CTA v mod P of the set running the phase, a whole-grid stage's on CTA
+// v mod grid), and every stage reads the links through L2 only (their lines
+// in an SM's L1 may be stale after a barrier), so the links, the counters
+// and the measurements have the bits of the launched path.
 SUN_DEV unsigned long long global_ns()
 {
     unsigned long long t;
@@ -1324,9 +1325,9 @@ SUN_DEV unsigned wait_count(const unsigned* count, unsigned target, int* status,
     return c;
 }
 // The waits of one update phase of a resident launch: `pre` the arrival
-// count at which the phase two back is complete (before any staple), `dep`
-// the count at which the previous phase is complete (before the staple of
-// its direction); 0: nothing to wait for.  Called by all lanes of a warp at
+// count at which the phase two back is complete (before any staple),
+// `dep_target` the count at which the previous phase is complete (before
+// the staple of its direction); 0: nothing to wait for.  Called by all lanes of a warp at
 // once: lane 0 polls (unless the CTA has seen the count already, *seen),
 // records the count seen, and the warp proceeds together.
 struct ResidentDep {
@@ -1337,9 +1338,15 @@ struct ResidentDep {
     unsigned* seen;
     SUN_DEV void wait_for(unsigned target) const
     {
-        if ((threadIdx.x & 31) == 0 && *reinterpret_cast<volatile unsigned*>(seen) < target) {
-            const unsigned c = wait_count(count, target, status, wait_ns);
-            if (c) atomicMax(seen, c);
+        if ((threadIdx.x & 31) == 0) {
+            if (*reinterpret_cast<volatile unsigned*>(seen) >= target) {
+                // another warp saw the count (its acquire fence, then the
+                // write of *seen); this fence makes the read an acquire
+                __threadfence_block();
+            } else {
+                const unsigned c = wait_count(count, target, status, wait_ns);
+                if (c) atomicMax(seen, c);
+            }
         }
         __syncwarp();
     }
