@@ -148,8 +148,8 @@ struct sun_ctx {
     // never, 1 whenever the lattice and launch shapes allow
     // (SUN_B200_RESIDENT).  Measured on B200, 1 HB + 4 OR with both
     // observables per sweep, us per sweep resident / captured graph: SU(3)
-    // FP32 8^4 189 / 206 (full links), 191 / 195 (12-parameter), 12^4
-    // 207 / 233; slower for FP64 (SU(3) 8^4 232 / 200, 12^4 297 / 268),
+    // FP32 8^4 188 / 200 (full links), 190 / 189 (12-parameter), 12^4
+    // 206 / 226; slower for FP64 (SU(3) 8^4 230 / 194, 12^4 297 / 268),
     // SU(2) (8^4 131 / 111), SU(4) (8^4 271 / 224) and from 16^4 up.
     int resident = -1;
     long long resident_max_halfv = 16384;

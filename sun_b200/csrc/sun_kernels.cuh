@@ -1504,9 +1504,10 @@ __global__ void __launch_bounds__(128) k_sweeps_resident(ResidentArgs a)
         prev = done;
         done += gridDim.x;
         if (!cta_wait(a, done, &seen)) return;
+        // finalized by two CTAs of set 1, which starts the next sweep second;
         // the partials are written again only after the next sweep's
         // barriers, which these CTAs reach after their finalize
-        if (blockIdx.x == 0 && threadIdx.x < 32) finalize_partials(a.partials, 0, a.plaq.nblocks, 2, a.out_plaq + 2 * sw);
+        if (blockIdx.x == P && threadIdx.x < 32) finalize_partials(a.partials, 0, a.plaq.nblocks, 2, a.out_plaq + 2 * sw);
         if (blockIdx.x == gridDim.x - 1 && threadIdx.x < 32) finalize_partials(ppart, 0, a.poly.nblocks, 2, a.out_poly + 2 * sw);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
