@@ -78,8 +78,18 @@ SUN_DEV void shifted(const Geom& g, const int x[4], int d, int s, int y[4])
 // N >= 4 in FP32: a 168-register cap (3 CTAs per SM) measured 18-28 % faster
 // than the uncapped kernels (208-255 registers, 1-2 CTAs) at 24^4; FP64 and
 // N = 2 are fastest uncapped.
+// Per mode (SUN_OCC_SUN_OR / _HB): a 128-register cap (4 CTAs) measured
+// slower for SU(4) FP32, overrelaxation 24^4 49.2 against 43.1 us per
+// launch, heatbath 71.8 against 60.5 us (spills).
+#ifndef SUN_OCC_SUN_OR
+#define SUN_OCC_SUN_OR 3
+#endif
+#ifndef SUN_OCC_SUN_HB
+#define SUN_OCC_SUN_HB 3
+#endif
 template <int N, class R, int MODE, int LAYOUT> struct UpdateOccupancy {
-    static constexpr int min_blocks = (N >= 4 && sizeof(R) == 4) ? 3 : 1;
+    static constexpr int min_blocks =
+        (N >= 4 && sizeof(R) == 4) ? (MODE == MODE_OR ? SUN_OCC_SUN_OR : SUN_OCC_SUN_HB) : 1;
 };
 template <class R, int MODE, int LAYOUT> struct UpdateOccupancy<3, R, MODE, LAYOUT> {
     static constexpr bool f32 = sizeof(R) == 4;
