@@ -185,9 +185,10 @@ sun_status sun_link_trace_det(sun_lattice *lat, double out[4], void *stream);
 sun_status sun_plaquette(sun_lattice *lat, double out[2], void *stream);
 /* The plaquette for callers that cannot allocate device memory (no
  * counterpart in the reference).  sun_plaquette() lets the library
- * cudaMalloc its reduction scratch on first use; code capturing a CUDA graph,
- * applications that own all device memory through their own pool, and hosts
- * with a fixed memory budget cannot allow that.  This entry point allocates
+ * cudaMalloc its reduction scratch on first use; applications that own all
+ * device memory through their own pool, hosts with a fixed memory budget and
+ * loops that cannot afford the synchronisation of a later cudaFree cannot
+ * allow that.  This entry point allocates
  * nothing: its scratch is a fixed 2 MiB array compiled into the library
  * (held on every GPU that loads it), so lattices of at most 8,388,608 sites
  * are accepted and larger ones are rejected with SUN_ERR_CAPACITY.

@@ -3,11 +3,11 @@
 //
 // sun_plaquette() keeps its per-CTA partial sums and its result in buffers
 // the library allocates with cudaMalloc on first use.  Some callers cannot
-// let a library allocate: code running inside a CUDA graph being captured
-// (cudaMalloc is not a capturable operation), applications that hand all
-// device memory to their own pool or arena and forbid allocations behind
-// their back, and embedded/real-time hosts with a fixed memory budget set at
-// start-up.  sun_plaquette_noalloc() serves them: the same measurement, with
+// let a library allocate: applications that hand all device memory to their
+// own pool or arena and forbid allocations behind their back, embedded and
+// real-time hosts with a fixed memory budget set at start-up, and loops that
+// cannot afford the device-wide synchronisation a library's later cudaFree
+// brings.  sun_plaquette_noalloc() serves them: the same measurement, with
 // its scratch in a fixed array compiled into this library.
 //
 // The scratch is g_plaq_scratch below: 4 doubles per CTA of 128 sites, for

@@ -1,8 +1,9 @@
 """The allocation-free plaquette entry point, sun_plaquette_noalloc.
 
-It exists for callers that cannot let a library call cudaMalloc: code that
-is capturing a CUDA graph, applications whose device memory all belongs to
-their own pool, and hosts with a fixed memory budget.  Its scratch is a fixed
+It exists for callers that cannot let a library call cudaMalloc:
+applications whose device memory all belongs to their own pool, hosts with a
+fixed memory budget, and loops that cannot afford the synchronisation of a
+later cudaFree.  Its scratch is a fixed
 array compiled into the library; these tests call it through the C ABI and
 check it against the allocating sun_plaquette on two calls in a row.
 
