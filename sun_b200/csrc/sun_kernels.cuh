@@ -170,16 +170,18 @@ SUN_DEV void update_site(const Geom& g, const LatDev& L, int id, int parity, int
         const int sz = (lex_step(ldn, xm, Xm, Sm, 1) >> 1) + parity * H;  // x - nu + mu
         Mat<N, R> A, B, C;
         if constexpr (N == 3 && LAYOUT == L_SOA12) {
-            // 12-parameter links: a product of two SU(3) links is SU(3), so
-            // only its rows 0, 1 are multiplied out (from the stored rows of
-            // the left factor, which is not rebuilt) and row 2 is rebuilt as
-            // conj(row0 x row1) -- 36 fewer real FMAs per staple
+            // 12-parameter links: a product of SU(3) links is SU(3), so only
+            // its rows 0, 1 are multiplied out (from the stored rows of the
+            // left factor, which is not rebuilt) and row 2 is rebuilt as
+            // conj(row0 x row1).  Up: rows 0, 1 of the whole staple from
+            // rows 0, 1 of U_nu(x) U_mu(x+nu), then its row 2, then added
             IO::load_rows_f(ld, sx + nu * V, stride, A);
             IO::load_f(ld, syp + mu * V, stride, B);
             mmul_rows01(A, B, C);
-            rebuild12(C);
             IO::load_f(ld, sxpmu + nu * V, stride, A);
-            macc_nd(C, A, S);
+            mmul_nd_rows01(C, A, B);
+            rebuild12(B);
+            madd(S, B);
             // down: U_nu(x-nu)^dagger [U_mu(x-nu) U_nu(x-nu+mu)]
             IO::load_rows_f(ld, sy + mu * V, stride, A);
             IO::load_f(ld, sz + nu * V, stride, B);
@@ -324,23 +326,24 @@ SUN_DEV void update_rows_warp(const Geom& g, const LatDev& L, int first, int par
         Mat<N, R> A, B;
         cx<R> a[N], c[N];
         if constexpr (N == 3 && LAYOUT == L_SOA12) {
-            // rows 0, 1 of the two-link product by lanes 0, 1 (lane 2 repeats
-            // row 0), row 2 rebuilt from them in every lane
+            // up: rows 0, 1 of the two-link product and then of the whole
+            // staple by lanes 0, 1 (lane 2 repeats row 0), the staple's row 2
+            // rebuilt from them in every lane
             cx<R> c0[3], c1[3], c2[3];
             IO::template load_rows<LD_CG>(base, sx + nu * V, stride, A);
             IO::template load<LD_CG>(base, syp + mu * V, stride, B);
             mrow<3, R, 2>(A, r, a);
             rmul<3, R>(a, B, c);
+            IO::template load<LD_CG>(base, sxpmu + nu * V, stride, A);
+            rmul_nd<3, R>(c, A, a);
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-                c0[j] = shfl_cx(c[j], lead);
-                c1[j] = shfl_cx(c[j], lead + 1);
+                c0[j] = shfl_cx(a[j], lead);
+                c1[j] = shfl_cx(a[j], lead + 1);
             }
             rebuild12_row<R>(c0, c1, c2);
 #pragma unroll
-            for (int j = 0; j < 3; ++j) c[j] = r == 0 ? c0[j] : (r == 1 ? c1[j] : c2[j]);
-            IO::template load<LD_CG>(base, sxpmu + nu * V, stride, A);
-            racc_nd<3, R>(c, A, Sr);
+            for (int j = 0; j < 3; ++j) Sr[j] = Sr[j] + (r == 0 ? c0[j] : (r == 1 ? c1[j] : c2[j]));
             // down: U_nu(x-nu)^dagger [U_mu(x-nu) U_nu(x-nu+mu)], the product
             // needed whole
             IO::template load_rows<LD_CG>(base, sy + mu * V, stride, A);

@@ -171,6 +171,27 @@ template <class R> SUN_HD void mmul_rows01(const Mat<3, R>& A, const Mat<3, R>& 
             C.e[i][j] = s;
         }
 }
+// rows 0 and 1 of C = A B^dagger (only rows 0, 1 of A are read)
+template <class R> SUN_HD void mmul_nd_rows01(const Mat<3, R>& A, const Mat<3, R>& B, Mat<3, R>& C)
+{
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            cx<R> s = mkc<R>(0, 0);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) s = cfma_nc(A.e[i][k], B.e[j][k], s);
+            C.e[i][j] = s;
+        }
+}
+// S += P
+template <int N, class R> SUN_HD void madd(Mat<N, R>& S, const Mat<N, R>& P)
+{
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j < N; ++j) S.e[i][j] = S.e[i][j] + P.e[i][j];
+}
 // -- one row of the products above, for kernels that spread a matrix over N
 // lanes (lane i owns row i).  Element (i, j) is formed by exactly the same
 // operations, in the same order, as in the whole-matrix routine it names, so
@@ -207,6 +228,17 @@ template <int N, class R> SUN_DEV void rmul(const cx<R> a[N], const Mat<N, R>& B
         cx<R> s = a[0] * B.e[0][j];
 #pragma unroll
         for (int k = 1; k < N; ++k) s = cfma(a[k], B.e[k][j], s);
+        c[j] = s;
+    }
+}
+// row i of A B^dagger from row i of A (a) -- mmul_nd, mmul_nd_rows01
+template <int N, class R> SUN_DEV void rmul_nd(const cx<R> a[N], const Mat<N, R>& B, cx<R> c[N])
+{
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        cx<R> s = mkc<R>(0, 0);
+#pragma unroll
+        for (int k = 0; k < N; ++k) s = cfma_nc(a[k], B.e[j][k], s);
         c[j] = s;
     }
 }
