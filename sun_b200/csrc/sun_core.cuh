@@ -196,7 +196,9 @@ template <class R, class Stream> SUN_DEV void su2_draw(R al, Stream& st, R a[4])
 // block from U and S like the reference; N >= 4 does the same (the
 // reference keeps M = U S^dagger and updates it with U, which needs N^2 more
 // live complex numbers); N = 2 keeps M.
-template <int N, class R, class Stream>
+// ROW2 false (SU(3) 12-parameter links, whose row 2 is not stored): the
+// last subgroup, (0, 2), rotates row 0 only and row 2 is left as it was.
+template <int N, class R, class Stream, bool ROW2 = true>
 SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, Stream& st)
 {
     if constexpr (N == 3) {
@@ -217,7 +219,8 @@ SUN_DEV void heatbath_update(Mat<N, R>& U, const Mat<N, R>& S, R beta_over_n, St
             su2_mul_udag(a, r, c);
             if (b == 0) su2_apply<N, R>(U, 0, 1, c);
             else if (b == 1) su2_apply<N, R>(U, 1, 2, c);
-            else su2_apply<N, R>(U, 0, 2, c);
+            else if (ROW2) su2_apply<N, R>(U, 0, 2, c);
+            else su2_apply_row_p<N, R>(U, 0, 2, c);
         }
     } else if constexpr (N >= 4) {
         // each block of U S^dagger recomputed from U and S instead of
@@ -273,7 +276,8 @@ template <class R> SUN_DEV void su2_overrelax_element(const R r[4], R c[4])
     c[3] = t * r[3];
 }
 
-template <int N, class R> SUN_DEV void overrelax_update(Mat<N, R>& U, const Mat<N, R>& S)
+// ROW2: as in heatbath_update.
+template <int N, class R, bool ROW2 = true> SUN_DEV void overrelax_update(Mat<N, R>& U, const Mat<N, R>& S)
 {
     if constexpr (N >= 3) {
         // blocks recomputed from U and S (for N >= 4 instead of the
@@ -284,7 +288,8 @@ template <int N, class R> SUN_DEV void overrelax_update(Mat<N, R>& U, const Mat<
             R r[4], c[4];
             su2_block_US<N, R>(U, S, p, q, r);
             su2_overrelax_element(r, c);
-            su2_apply<N, R>(U, p, q, c);
+            if (ROW2 || N != 3 || b + 1 < SubGroup<N>::count) su2_apply<N, R>(U, p, q, c);
+            else su2_apply_row_p<N, R>(U, p, q, c);
         }
     } else {
         Mat<N, R> M;

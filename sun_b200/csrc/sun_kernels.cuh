@@ -210,19 +210,19 @@ SUN_DEV void update_site(const Geom& g, const LatDev& L, int id, int parity, int
     IO::load_f(ld, own, stride, U);
     if constexpr (N == 3 && LAYOUT == L_SOA12) unit_row2<R>(U);
     if constexpr (MODE == MODE_OR) {
-        overrelax_update<N, R>(U, S);
+        overrelax_update<N, R, !(N == 3 && LAYOUT == L_SOA12)>(U, S);
     } else {
         const R bon = (R)L.beta_over_n;
         if constexpr (MODE == MODE_HB) {
             PhiloxStream<R> ph;
             ph.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
-            heatbath_update<N, R>(U, S, bon, ph);
+            heatbath_update<N, R, PhiloxStream<R>, !(N == 3 && LAYOUT == L_SOA12)>(U, S, bon, ph);
         } else {
             InjectedStream<R> is;
             is.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
             is.left = inj.stride;
             is.err = inj.err;
-            heatbath_update<N, R>(U, S, bon, is);
+            heatbath_update<N, R, InjectedStream<R>, !(N == 3 && LAYOUT == L_SOA12)>(U, S, bon, is);
         }
     }
     IO::store_f(st, own, stride, U);
@@ -393,19 +393,19 @@ SUN_DEV void update_rows_warp(const Geom& g, const LatDev& L, int first, int par
     IO::template load<LD_CG>(wbase, own, stride, U);
     if constexpr (N == 3 && LAYOUT == L_SOA12) unit_row2<R>(U);
     if constexpr (MODE == MODE_OR) {
-        overrelax_update<N, R>(U, S);
+        overrelax_update<N, R, !(N == 3 && LAYOUT == L_SOA12)>(U, S);
     } else {
         const R bon = (R)L.beta_over_n;
         if constexpr (MODE == MODE_HB) {
             PhiloxStream<R> st;
             st.init(L.seed, (uint32_t)lex, (uint32_t)mu, L.state[0] + hb_offset);
-            heatbath_update<N, R>(U, S, bon, st);
+            heatbath_update<N, R, decltype(st), !(N == 3 && LAYOUT == L_SOA12)>(U, S, bon, st);
         } else {
             InjectedStream<R> st;
             st.p = inj.u + ((size_t)lex * 4 + mu) * inj.stride;
             st.left = inj.stride;
             st.err = inj.err;
-            heatbath_update<N, R>(U, S, bon, st);
+            heatbath_update<N, R, decltype(st), !(N == 3 && LAYOUT == L_SOA12)>(U, S, bon, st);
         }
     }
     if (valid && r == 0) IO::store(wbase, own, stride, U);

@@ -502,6 +502,14 @@ template <int N, class R> SUN_DEV void su2_apply(Mat<N, R>& L, int p, int q, con
         L.e[q][j] = cfma(a11, uq, a10 * up);
     }
 }
+// row p only of su2_apply (the same operations), for a last subgroup whose
+// row q is not needed afterwards
+template <int N, class R> SUN_DEV void su2_apply_row_p(Mat<N, R>& L, int p, int q, const R b[4])
+{
+    const cx<R> a00 = mkc(b[0], b[3]), a01 = mkc(b[2], b[1]);
+#pragma unroll
+    for (int j = 0; j < N; ++j) L.e[p][j] = cfma(a01, L.e[q][j], a00 * L.e[p][j]);
+}
 // a * r^dagger on quaternion 4-vectors -- mulsu2UVDagger (msu2.h:212-219)
 template <class R> SUN_DEV void su2_mul_udag(const R a[4], const R r[4], R b[4])
 {
