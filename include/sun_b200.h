@@ -148,9 +148,9 @@ sun_status sun_sweep(sun_lattice *lat, int n_hb, int n_or, int n_sweeps, void *s
  * spatial and temporal plaquette after sweep i; poly[2i], poly[2i+1]:
  * Polyakov loop; host arrays of 2 n_sweeps doubles, either may be NULL.
  * A small SU(3) FP32 lattice (at most 16384 half-sites; SUN_B200_RESIDENT=
- * 0|1|auto, SUN_B200_RESIDENT_MAX_HALFV) runs all n_sweeps in one
- * cooperative launch whose grid barriers replace the launch boundaries,
- * with the same results; a barrier wait that runs out (one second) returns
+ * 0|1|auto, SUN_B200_RESIDENT_MAX_HALFV) runs its sweeps in cooperative
+ * launches of up to 256 sweeps whose grid barriers replace the launch
+ * boundaries, with the same results; a barrier wait that runs out (one second) returns
  * SUN_ERR_DEVICE_FLAG. */
 sun_status sun_sweep_measure(sun_lattice *lat, int n_hb, int n_or, int n_sweeps, double *plaq, double *poly,
                              void *stream);

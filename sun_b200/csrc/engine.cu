@@ -1166,7 +1166,10 @@ static bool solo_measure_graph(sun_lattice* l, Group& g, int n_hb, int n_or, siz
     return true;
 }
 
-// sun_sweep_measure as one cooperative launch (k_sweeps_resident), for a
+// sweeps per resident launch at most
+constexpr int kResidentChunk = 256;
+
+// sun_sweep_measure in cooperative launches (k_sweeps_resident), for a
 // lattice whose launched phases are latency-bound.  Returns false, having
 // launched nothing, when the lattice, the launch shapes or the stream do not
 // allow it.
@@ -1199,17 +1202,13 @@ static bool resident_sweeps(sun_lattice* l, Group& g, int n_hb, int n_or, int n_
     g.partials.ensure(sizeof(double) * 4 * (size_t)(vp.nblocks + vl.nblocks));
     c->res_sync.ensure(4 * sizeof(unsigned));
     c->res_out.ensure(sizeof(double) * 4 * (size_t)n_sweeps);
-    ck(cudaMemsetAsync(c->res_sync.p, 0, 4 * sizeof(unsigned), s), "barrier reset");
     ResidentArgs a{};
     a.upd = upd;
     a.plaq = vp;
     a.poly = vl;
     a.n_hb = n_hb;
     a.n_or = n_or;
-    a.n_sweeps = n_sweeps;
     a.partials = reinterpret_cast<double*>(g.partials.p);
-    a.out_plaq = reinterpret_cast<double*>(c->res_out.p);
-    a.out_poly = a.out_plaq + 2 * (size_t)n_sweeps;
     a.bar = reinterpret_cast<unsigned*>(c->res_sync.p);
     a.status = reinterpret_cast<int*>(a.bar + 2);
     a.wait_ns = c->barrier_wait_ns;
@@ -1217,15 +1216,27 @@ static bool resident_sweeps(sun_lattice* l, Group& g, int n_hb, int n_or, int n_
     // two sets of CTAs that take the phases in turn, each covering the
     // update's CTAs (several per resident CTA when they do not all fit)
     const int grid = 2 * std::max(1, std::min(cap_ctas / 2, upd.nblocks));
-    OPS_CALL(g.N, sweeps_resident, g.fp64, g.layout, rows, a, grid, s);
+    // at most kResidentChunk sweeps per launch, so no launch runs long; each
+    // continues from the counters the one before left, and its status is
+    // read before the next starts
+    double* out_p = reinterpret_cast<double*>(c->res_out.p);
+    double* out_l = out_p + 2 * (size_t)n_sweeps;
+    for (int done = 0; done < n_sweeps; done += kResidentChunk) {
+        ck(cudaMemsetAsync(c->res_sync.p, 0, 4 * sizeof(unsigned), s), "barrier reset");
+        a.n_sweeps = std::min(kResidentChunk, n_sweeps - done);
+        a.out_plaq = out_p + 2 * (size_t)done;
+        a.out_poly = out_l + 2 * (size_t)done;
+        OPS_CALL(g.N, sweeps_resident, g.fp64, g.layout, rows, a, grid, s);
+        int status = 0;
+        ck(cudaMemcpyAsync(&status, a.status, sizeof(int), cudaMemcpyDeviceToHost, s), "status copy");
+        ck(cudaStreamSynchronize(s), "resident sweeps");
+        if (status)
+            fail(SUN_ERR_DEVICE_FLAG, "a grid barrier wait of the resident sweeps ran out (limit %llu ns); the links "
+                 "are left part-updated", (unsigned long long)c->barrier_wait_ns);
+    }
     std::vector<double> h(4 * (size_t)n_sweeps);
-    int status = 0;
     ck(cudaMemcpyAsync(h.data(), c->res_out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s), "copy");
-    ck(cudaMemcpyAsync(&status, a.status, sizeof(int), cudaMemcpyDeviceToHost, s), "status copy");
     ck(cudaStreamSynchronize(s), "resident sweeps");
-    if (status)
-        fail(SUN_ERR_DEVICE_FLAG, "a grid barrier wait of the resident sweeps ran out (limit %llu ns); the links "
-             "are left part-updated", (unsigned long long)c->barrier_wait_ns);
     const double np = 3.0 * l->p.ncolors * (double)L.V, nl = (double)l->p.ncolors * L.X[0] * L.X[1] * L.X[2];
     for (int i = 0; i < 2 * n_sweeps; ++i) {
         if (plaq) plaq[i] = h[i] / np;

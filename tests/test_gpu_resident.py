@@ -103,6 +103,28 @@ def test_resident_sweeps_match_launched_path(case):
         off.close()
 
 
+def test_resident_calls_longer_than_one_launch():
+    """300 sweeps take two resident launches (256 sweeps at most each): the
+    second continues from the first's counters, with the launched path's
+    links and per-sweep values."""
+    from sun_b200 import SweepMeasure
+    case = CASES[2]
+    on = _context(SUN_B200_RESIDENT="1")
+    off = _context(SUN_B200_RESIDENT="0")
+    try:
+        a, b = _lattice(on, case), _lattice(off, case)
+        pa, la = SweepMeasure(a, 1, 4, 300)
+        pb, lb = SweepMeasure(b, 1, 4, 300)
+        assert np.array_equal(pa, pb) and np.array_equal(la, lb)
+        assert np.array_equal(a.get_image(), b.get_image())
+        assert a.rng_state() == b.rng_state()
+        a.Release()
+        b.Release()
+    finally:
+        on.close()
+        off.close()
+
+
 def test_resident_barrier_wait_runs_out_and_context_recovers():
     from sun_b200 import PlaquetteCUB, SweepMeasure
     from sun_b200._native import SunError, lib
